@@ -1,0 +1,226 @@
+/*
+ * raptr_b200 -- C ABI of the B200 (sm_100a) reconstruction hot path of raptr.
+ *
+ * Plain C types only: device buffers are raw pointers allocated by the caller
+ * (cudaMalloc or any allocator), sizes are int64_t, a CUDA stream is passed
+ * as `void *` (a cudaStream_t; NULL = the legacy default stream).  Every call
+ * is stream-ordered unless documented otherwise, returns a raptr_status and
+ * never aborts; raptr_last_error() describes the last failure of the calling
+ * thread.
+ *
+ * Reference interfaces replaced (paths relative to the raptr source tree):
+ *   raptr_workqueue        getWorkqueue            src/getWorkqueue.hpp:149-155, :207-212
+ *   raptr_rays             RandRayGen              src/RayGenerators.hpp:36-67
+ *   raptr_sm_build         systemMatrixCalculation src/wrappers.hpp:185-196
+ *                          (kernel getSystemMatrix src/getSystemMatrixDeviceOnly.cu:357-384,
+ *                           cooSort src/cooSort.hpp:75-99,
+ *                           convertCoo2Csr src/cusparseWrapper.hpp:53-60,
+ *                           convertCsr2Ecsr src/convertCsr2Ecsr.hpp:51-64)
+ *   raptr_coo2csr          convertCoo2Csr          src/cusparseWrapper.hpp:53-60
+ *   raptr_csr2ecsr         convertCsr2Ecsr         src/convertCsr2Ecsr.hpp:51-64
+ *   raptr_spmv             CSRmv<float>            src/csrmv.hpp:61-66, :72-83
+ *   raptr_divides          divides                 src/mlemOperations.hpp:44-54
+ *   raptr_divides_multiplies dividesMultiplies     src/mlemOperations.hpp:88-104
+ *   raptr_scales           scales                  src/mlemOperations.hpp:146-153
+ *   raptr_sum              sum                     src/mlemOperations.hpp:163-169
+ *   raptr_mlem             MLEM loop               src/tests/reco.cu:229-321
+ *   raptr_reco_host        reco main flow          src/tests/reco.cu:53-352
+ */
+#ifndef RAPTR_B200_H
+#define RAPTR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RAPTR_ABI_VERSION 1
+
+typedef enum raptr_status {
+  RAPTR_OK = 0,
+  RAPTR_ERR_INVALID = 1,     /* bad argument (null pointer, size, geometry)        */
+  RAPTR_ERR_CUDA = 2,        /* a CUDA runtime call failed                          */
+  RAPTR_ERR_CAPACITY = 3,    /* caller buffer too small; required size returned     */
+  RAPTR_ERR_OVERFLOW = 4,    /* an internal per-row table overflowed (after retry)  */
+  RAPTR_ERR_NOMEM = 5,       /* device allocation failed                            */
+  RAPTR_ERR_UNSUPPORTED = 6  /* feature not available for these arguments           */
+} raptr_status;
+
+/* Scanner geometry.  Field meaning and units as in DefaultVoxelGrid
+ * (src/VoxelGrid.hpp:151-176: grid origin, voxel pitch, voxel counts) and
+ * DefaultMeasurementSetup (src/MeasurementSetup.hpp:181-220).  Voxel linear
+ * id = ix*ny*nz + iy*nz + iz (src/VoxelGridLinIndex.hpp:74-80); channel
+ * linear id = (((ida*n0z + id0z)*n0y + id0y)*n1z + id1z)*n1y + id1y
+ * (src/MeasurementSetupLinIndex.hpp:82-91). */
+typedef struct raptr_geom {
+  float grid_o[3];
+  float grid_d[3];
+  int32_t grid_n[3];
+  float pos0x, pos1x;
+  int32_t na, n0z, n0y, n1z, n1y;
+  float da, segx, segy, segz;
+} raptr_geom;
+
+/* A per-geometry device context: the per-angle sine/cosine table, the
+ * device it lives on and reusable scratch.  Contexts are independent (no
+ * global state), so geometries can be served side by side.  A context may
+ * be used from one host thread at a time. */
+typedef struct raptr_ctx raptr_ctx;
+
+/* A system matrix held by the library in device memory (CSR, int64 row
+ * pointers, int32 columns, float values). */
+typedef struct raptr_matrix raptr_matrix;
+
+int raptr_abi_version(void);
+const char* raptr_last_error(void);
+
+raptr_status raptr_ctx_create(const raptr_geom* geom, int device, raptr_ctx** out);
+raptr_status raptr_ctx_destroy(raptr_ctx* ctx);
+int64_t raptr_ctx_num_channels(const raptr_ctx* ctx);
+int64_t raptr_ctx_num_voxels(const raptr_ctx* ctx);
+
+/* ---- candidate search (getWorkqueue) ------------------------------------ */
+
+/* Enclosing-cylinder candidates (channel, voxel) of the listed channels in
+ * the reference's scan order (list-major, voxel-minor), starting at the
+ * cursor (*list_id, *vxl_id) and returning at most max_out entries.  On
+ * return the cursor points one voxel past the last entry returned (next list
+ * entry at the end of the grid; (n_list, 0) when exhausted), as
+ * getWorkqueueEntry leaves it (src/getWorkqueue.hpp:53-133).  d_cnl_out and
+ * d_vxl_out hold max_out entries.  Synchronises the stream (the count and
+ * cursor are host values). */
+raptr_status raptr_workqueue(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int64_t* list_id,
+                             int64_t* vxl_id, int64_t max_out, int32_t* d_cnl_out, int32_t* d_vxl_out,
+                             int64_t* n_found, void* stream);
+
+/* Number of candidates of each listed channel (d_counts: n_list int64). */
+raptr_status raptr_candidate_counts(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int64_t* d_counts,
+                                    void* stream);
+
+/* ---- rays ------------------------------------------------------------------ */
+
+/* Endpoints of rays [0, nrays) of each listed channel: d_rays holds
+ * n_list*nrays*6 floats (x0,y0,z0,x1,y1,z1).  Uniforms come from
+ * Philox4x32-10 with key (seed, channel) and counter (ray, 0|1, 0, 0); the
+ * reference draws them from curand XORWOW instead (src/RayGenerators.hpp:44). */
+raptr_status raptr_rays(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int32_t nrays, uint32_t seed,
+                        float* d_rays, void* stream);
+
+/* ---- system matrix --------------------------------------------------------- */
+
+#define RAPTR_SM_KEEP_ZEROS 1 /* keep every candidate, also exact zeros (the reference's COO structure) */
+
+/* Rows of the system matrix for the listed channels, row i <-> d_cnl_ids[i]
+ * (the reference's ECSR row space).  Element (i, v) = mean over rays of the
+ * intersection length of ray r with voxel v, for every voxel v that passes
+ * the enclosing-cylinder test; exact zeros are dropped unless
+ * RAPTR_SM_KEEP_ZEROS.  Columns ascend within a row.  Rays come from
+ * d_rays (n_list*nrays*6 floats) when non-null, else from the Philox stream
+ * of raptr_rays.
+ *
+ * Output goes to caller buffers: d_row_ptr (n_list+1 int64), d_col/d_val
+ * (capacity entries).  If the matrix has more than `capacity` entries the
+ * call returns RAPTR_ERR_CAPACITY with *nnz_out = the required count and
+ * the row pointers filled (call again with a larger buffer).  Synchronises
+ * the stream. */
+raptr_status raptr_sm_build(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int32_t nrays, uint32_t seed,
+                            const float* d_rays, int32_t flags, int64_t capacity, int64_t* d_row_ptr, int32_t* d_col,
+                            float* d_val, int64_t* nnz_out, void* stream);
+
+/* Same build into a matrix allocated and owned by the library (resident in
+ * HBM until raptr_matrix_destroy). */
+raptr_status raptr_sm_build_alloc(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int32_t nrays,
+                                  uint32_t seed, const float* d_rays, int32_t flags, raptr_matrix** out,
+                                  void* stream);
+raptr_status raptr_matrix_info(const raptr_matrix* A, int64_t* m, int64_t* n, int64_t* nnz, int64_t** d_row_ptr,
+                               int32_t** d_col, float** d_val);
+raptr_status raptr_matrix_destroy(raptr_matrix* A);
+
+/* ---- sparse formats --------------------------------------------------------- */
+
+/* Row pointers (m+1 int64) from sorted COO row indices (nnz int32). */
+raptr_status raptr_coo2csr(const int32_t* d_rows, int64_t nnz, int64_t m, int64_t* d_row_ptr, void* stream);
+
+/* ECSR row pointers: d_ecsr[i] = d_csr[d_yrow[i]], d_ecsr[nnzr] = d_csr[m]. */
+raptr_status raptr_csr2ecsr(int64_t* d_ecsr, const int32_t* d_yrow, int64_t nnzr, const int64_t* d_csr, int64_t m,
+                            void* stream);
+
+/* ---- SpMV ---------------------------------------------------------------- */
+
+#define RAPTR_OP_N 0 /* y = alpha*A*x   + beta*y  (forward projection) */
+#define RAPTR_OP_T 1 /* y = alpha*A^T*x + beta*y  (back projection)    */
+
+/* The CSRmv contract (src/csrmv.hpp:31-66) on an m x n CSR matrix with
+ * int64 row pointers.  beta == 0 does not read y. */
+raptr_status raptr_spmv(int32_t op, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                        const float* d_val, float alpha, const float* d_x, float beta, float* d_y, void* stream);
+
+/* ---- element-wise MLEM operations --------------------------------------- */
+
+raptr_status raptr_divides(float* d_res, const float* d_dividend, const float* d_divisor, int64_t n, void* stream);
+raptr_status raptr_divides_multiplies(float* d_res, const float* d_a, const float* d_b, const float* d_c, int64_t n,
+                                      void* stream);
+raptr_status raptr_scales(float* d_x, float alpha, int64_t n, void* stream);
+/* Sum of d_x, accumulated in double; synchronises the stream. */
+raptr_status raptr_sum(const float* d_x, int64_t n, double* sum_out, void* stream);
+
+/* ---- sensitivity and MLEM ------------------------------------------------- */
+
+/* Column sums of A in double (d_s64, n entries, overwritten) and, when
+ * d_s32 is non-null, the same image normalised to sum 1 in float. */
+raptr_status raptr_sensitivity(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                               const float* d_val, double* d_s64, float* d_s32, void* stream);
+
+typedef struct raptr_mlem_opts {
+  int32_t use_graph;   /* capture the iteration loop in a CUDA graph            */
+  double* h_loglik;    /* optional: per-iteration Poisson log-likelihood (FP64)  */
+} raptr_mlem_opts;
+
+/* n_iter MLEM iterations in the order of src/tests/reco.cu:230-303:
+ * yt = A x; e = y / yt; c = A^T e; x = x*c/(s + (s==0)); x *= 1/sum(x).
+ * Rows of A correspond to d_y.  d_s is the normalised sensitivity.  d_x is
+ * updated in place.  One fused pass over A per iteration. */
+raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                        const float* d_val, const float* d_y, const float* d_s, float* d_x, int32_t n_iter,
+                        const raptr_mlem_opts* opts, void* stream);
+
+/* The two halves of one MLEM iteration, for callers that combine partial
+ * back projections across devices (row-sharded matrix):
+ *   raptr_mlem_project: d_c += A^T (d_y / (A d_x)) over the rows of this
+ *     shard (rows with y == 0 skipped); when d_ll is non-null, d_ll[0] +=
+ *     sum y*log(Ax) and d_ll[1] += sum Ax in FP64;
+ *   raptr_mlem_update: d_x = d_x*d_c/(d_s + (d_s==0)); d_x *= 1/sum(d_x);
+ *     d_c = 0.  d_acc is one double of device scratch. */
+raptr_status raptr_mlem_project(int64_t m, const int64_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                                const float* d_y, const float* d_x, float* d_c, double* d_ll, void* stream);
+raptr_status raptr_mlem_update(int64_t n, float* d_x, float* d_c, const float* d_s, double* d_acc, void* stream);
+
+/* ---- end-to-end ------------------------------------------------------------ */
+
+typedef struct raptr_reco_stats {
+  double build_ms;      /* system matrix build (all channels)            */
+  double sens_ms;       /* sensitivity                                   */
+  double iter_ms;       /* all MLEM iterations                           */
+  double total_ms;      /* whole call including copies                   */
+  int64_t nnz;          /* entries of the matrix                         */
+  int64_t h2d_bytes;    /* bytes copied host -> device                   */
+  int64_t d2h_bytes;    /* bytes copied device -> host                   */
+} raptr_reco_stats;
+
+/* The reco executable's flow from host buffers (src/tests/reco.cu:53-352):
+ * measured counts h_y over all channels of the geometry (dense, num_channels
+ * floats, zero = not measured), nrays rays per channel, n_iter iterations
+ * from h_x0 (num_voxels floats; null = uniform image normalised to sum 1),
+ * result in h_x (num_voxels floats).  The sensitivity is computed from the
+ * matrix of all channels (h_sens null) or taken from h_sens (num_voxels).
+ * The matrix is built once and kept resident for all iterations. */
+raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_y, int32_t nrays, uint32_t seed,
+                             int32_t n_iter, const float* h_sens, const float* h_x0, float* h_x,
+                             raptr_reco_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RAPTR_B200_H */

@@ -1,0 +1,381 @@
+"""raptr_b200: the reconstruction hot path of raptr (candidate search, Monte
+Carlo system matrix, CSR, MLEM) as hand-written sm_100a CUDA behind a C ABI
+(include/raptr_b200.h, libraptr_b200.so).
+
+This module is a thin ctypes layer over that library; PyTorch provides device
+memory and streams.  There is no CPU fallback: if the library is missing or
+no CUDA device is present the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from .config import FINE, FULL, SMALL, WORKLOADS, Geometry, epet_geometry, phantom, poisson_measurement
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libraptr_b200.so")
+
+RAPTR_OK = 0
+RAPTR_ERR_CAPACITY = 3
+OP_N = 0
+OP_T = 1
+SM_KEEP_ZEROS = 1
+
+STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "CAPACITY", 4: "OVERFLOW", 5: "NOMEM", 6: "UNSUPPORTED"}
+
+
+class RaptrError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"raptr status {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class raptr_geom(C.Structure):
+    _fields_ = [
+        ("grid_o", C.c_float * 3),
+        ("grid_d", C.c_float * 3),
+        ("grid_n", C.c_int32 * 3),
+        ("pos0x", C.c_float),
+        ("pos1x", C.c_float),
+        ("na", C.c_int32),
+        ("n0z", C.c_int32),
+        ("n0y", C.c_int32),
+        ("n1z", C.c_int32),
+        ("n1y", C.c_int32),
+        ("da", C.c_float),
+        ("segx", C.c_float),
+        ("segy", C.c_float),
+        ("segz", C.c_float),
+    ]
+
+
+class raptr_mlem_opts(C.Structure):
+    _fields_ = [("use_graph", C.c_int32), ("h_loglik", C.POINTER(C.c_double))]
+
+
+class raptr_reco_stats(C.Structure):
+    _fields_ = [
+        ("build_ms", C.c_double),
+        ("sens_ms", C.c_double),
+        ("iter_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("nnz", C.c_int64),
+        ("h2d_bytes", C.c_int64),
+        ("d2h_bytes", C.c_int64),
+    ]
+
+
+def geom_struct(g: Geometry) -> raptr_geom:
+    s = raptr_geom()
+    for i in range(3):
+        s.grid_o[i] = g.grid_o[i]
+        s.grid_d[i] = g.grid_d[i]
+        s.grid_n[i] = g.grid_n[i]
+    for f in ("pos0x", "pos1x", "na", "n0z", "n0y", "n1z", "n1y", "da", "segx", "segy", "segz"):
+        setattr(s, f, getattr(g, f))
+    return s
+
+
+_lib = None
+VP = C.c_void_p
+I64 = C.c_int64
+I32 = C.c_int32
+P64 = C.POINTER(C.c_int64)
+
+# name -> (restype, argtypes); every entry point of include/raptr_b200.h
+_SIGNATURES = {
+    "raptr_abi_version": (C.c_int, []),
+    "raptr_last_error": (C.c_char_p, []),
+    "raptr_ctx_create": (C.c_int, [C.POINTER(raptr_geom), C.c_int, C.POINTER(VP)]),
+    "raptr_ctx_destroy": (C.c_int, [VP]),
+    "raptr_ctx_num_channels": (I64, [VP]),
+    "raptr_ctx_num_voxels": (I64, [VP]),
+    "raptr_workqueue": (C.c_int, [VP, VP, I64, P64, P64, I64, VP, VP, P64, VP]),
+    "raptr_candidate_counts": (C.c_int, [VP, VP, I64, VP, VP]),
+    "raptr_rays": (C.c_int, [VP, VP, I64, I32, C.c_uint32, VP, VP]),
+    "raptr_sm_build": (C.c_int, [VP, VP, I64, I32, C.c_uint32, VP, I32, I64, VP, VP, VP, P64, VP]),
+    "raptr_sm_build_alloc": (C.c_int, [VP, VP, I64, I32, C.c_uint32, VP, I32, C.POINTER(VP), VP]),
+    "raptr_matrix_info": (C.c_int, [VP, P64, P64, P64, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP)]),
+    "raptr_matrix_destroy": (C.c_int, [VP]),
+    "raptr_coo2csr": (C.c_int, [VP, I64, I64, VP, VP]),
+    "raptr_csr2ecsr": (C.c_int, [VP, VP, I64, VP, I64, VP]),
+    "raptr_spmv": (C.c_int, [I32, I64, I64, VP, VP, VP, C.c_float, VP, C.c_float, VP, VP]),
+    "raptr_divides": (C.c_int, [VP, VP, VP, I64, VP]),
+    "raptr_divides_multiplies": (C.c_int, [VP, VP, VP, VP, I64, VP]),
+    "raptr_scales": (C.c_int, [VP, C.c_float, I64, VP]),
+    "raptr_sum": (C.c_int, [VP, I64, C.POINTER(C.c_double), VP]),
+    "raptr_sensitivity": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP]),
+    "raptr_mlem_project": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, VP, VP]),
+    "raptr_mlem_update": (C.c_int, [I64, VP, VP, VP, VP, VP]),
+    "raptr_mlem": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, I32, C.POINTER(raptr_mlem_opts), VP]),
+    "raptr_reco_host": (C.c_int, [C.POINTER(raptr_geom), C.c_int, VP, I32, C.c_uint32, I32, VP, VP, VP,
+                                  C.POINTER(raptr_reco_stats)]),
+}
+
+
+def lib():
+    """Loads libraptr_b200.so (built in-tree by raptr_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `python -m raptr_b200.build` (there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != RAPTR_OK:
+        raise RaptrError(status, lib().raptr_last_error().decode())
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("raptr_b200 needs a CUDA device (sm_100a); none is available")
+    return torch
+
+
+def _ptr(t) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _stream(stream=None) -> int:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+class _DeviceArray:
+    """Zero-copy __cuda_array_interface__ view of library-owned memory; keeps
+    its owner alive."""
+
+    def __init__(self, ptr: int, shape, typestr: str, owner):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+        self._owner = owner
+
+
+class Matrix:
+    """System matrix rows held by the library (CSR: int64 row_ptr, int32 col,
+    float32 val), resident in device memory."""
+
+    def __init__(self, handle: int, device: int):
+        self._h = VP(handle)
+        self.device = device
+        m, n, nnz = C.c_int64(), C.c_int64(), C.c_int64()
+        rp, col, val = VP(), VP(), VP()
+        _check(lib().raptr_matrix_info(self._h, C.byref(m), C.byref(n), C.byref(nnz), C.byref(rp), C.byref(col),
+                                       C.byref(val)))
+        self.m, self.n, self.nnz = m.value, n.value, nnz.value
+        torch = _torch()
+        dev = torch.device("cuda", device)
+        self.row_ptr = torch.as_tensor(_DeviceArray(rp.value, (self.m + 1,), "<i8", self), device=dev)
+        if self.nnz > 0:
+            self.col = torch.as_tensor(_DeviceArray(col.value, (self.nnz,), "<i4", self), device=dev)
+            self.val = torch.as_tensor(_DeviceArray(val.value, (self.nnz,), "<f4", self), device=dev)
+        else:
+            self.col = torch.zeros(0, dtype=torch.int32, device=dev)
+            self.val = torch.zeros(0, dtype=torch.float32, device=dev)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.raptr_matrix_destroy(h)
+            self._h = VP(0)
+
+    def to_numpy(self):
+        return self.row_ptr.cpu().numpy(), self.col.cpu().numpy(), self.val.cpu().numpy()
+
+
+class Context:
+    """Per-geometry device context (raptr_ctx)."""
+
+    def __init__(self, geom: Geometry, device: int = 0):
+        self.geom = geom
+        self.device = device
+        self._gs = geom_struct(geom)
+        h = VP()
+        _check(lib().raptr_ctx_create(C.byref(self._gs), device, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.raptr_ctx_destroy(h)
+            self._h = VP(0)
+
+    @property
+    def n_channels(self) -> int:
+        return lib().raptr_ctx_num_channels(self._h)
+
+    @property
+    def n_voxels(self) -> int:
+        return lib().raptr_ctx_num_voxels(self._h)
+
+    def _dev(self):
+        torch = _torch()
+        return torch.device("cuda", self.device)
+
+    def _list(self, cnl):
+        torch = _torch()
+        t = torch.as_tensor(cnl, dtype=torch.int32, device=self._dev())
+        return t.contiguous()
+
+    # -- candidate search ----------------------------------------------------
+    def workqueue(self, cnl, cursor: Tuple[int, int] = (0, 0), max_out: int = 1 << 20, stream=None):
+        """getWorkqueue: (cnl, vxl) candidates in scan order from `cursor`,
+        at most max_out; returns (cnl, vxl, new_cursor)."""
+        torch = _torch()
+        lst = self._list(cnl)
+        oc = torch.empty(max(max_out, 1), dtype=torch.int32, device=self._dev())
+        ov = torch.empty(max(max_out, 1), dtype=torch.int32, device=self._dev())
+        li, vi, nf = C.c_int64(cursor[0]), C.c_int64(cursor[1]), C.c_int64()
+        _check(lib().raptr_workqueue(self._h, _ptr(lst), lst.numel(), C.byref(li), C.byref(vi), max_out, _ptr(oc),
+                                     _ptr(ov), C.byref(nf), _stream(stream)))
+        n = nf.value
+        return oc[:n], ov[:n], (li.value, vi.value)
+
+    def candidate_counts(self, cnl, stream=None):
+        torch = _torch()
+        lst = self._list(cnl)
+        out = torch.empty(lst.numel(), dtype=torch.int64, device=self._dev())
+        _check(lib().raptr_candidate_counts(self._h, _ptr(lst), lst.numel(), _ptr(out), _stream(stream)))
+        return out
+
+    # -- rays and matrix -------------------------------------------------------
+    def rays(self, cnl, nrays: int, seed: int, stream=None):
+        torch = _torch()
+        lst = self._list(cnl)
+        out = torch.empty((lst.numel(), nrays, 6), dtype=torch.float32, device=self._dev())
+        _check(lib().raptr_rays(self._h, _ptr(lst), lst.numel(), nrays, seed, _ptr(out), _stream(stream)))
+        return out
+
+    def build(self, cnl, nrays: int, seed: int, rays=None, keep_zeros: bool = False, stream=None) -> Matrix:
+        """systemMatrixCalculation: rows for the listed channels, resident."""
+        lst = self._list(cnl)
+        rp = None
+        if rays is not None:
+            rays = rays.to(device=self._dev(), dtype=_torch().float32).contiguous()
+            assert rays.numel() == lst.numel() * nrays * 6
+            rp = _ptr(rays)
+        h = VP()
+        _check(lib().raptr_sm_build_alloc(self._h, _ptr(lst), lst.numel(), nrays, seed, rp,
+                                          SM_KEEP_ZEROS if keep_zeros else 0, C.byref(h), _stream(stream)))
+        return Matrix(h.value, self.device)
+
+    def build_into(self, cnl, nrays: int, seed: int, row_ptr, col, val, rays=None, keep_zeros=False, stream=None):
+        """raptr_sm_build into caller tensors; returns (status, nnz)."""
+        lst = self._list(cnl)
+        nnz = C.c_int64()
+        st = lib().raptr_sm_build(self._h, _ptr(lst), lst.numel(), nrays, seed, _ptr(rays),
+                                  SM_KEEP_ZEROS if keep_zeros else 0, 0 if col is None else col.numel(), _ptr(row_ptr),
+                                  _ptr(col), _ptr(val), C.byref(nnz), _stream(stream))
+        if st not in (RAPTR_OK, RAPTR_ERR_CAPACITY):
+            _check(st)
+        return st, nnz.value
+
+    def mlem(self, A: Matrix, y, s, x, niter: int, use_graph: bool = True, loglik: bool = False, stream=None):
+        """MLEM iterations in place on x; returns per-iteration log-likelihood or None."""
+        ll = (C.c_double * max(niter, 1))() if loglik else None
+        opts = raptr_mlem_opts(1 if use_graph else 0, C.cast(ll, C.POINTER(C.c_double)) if loglik else None)
+        _check(lib().raptr_mlem(self._h, A.m, A.n, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(y), _ptr(s),
+                                _ptr(x), niter, C.byref(opts), _stream(stream)))
+        return np.array(ll[:niter]) if loglik else None
+
+
+# -- context-free operations ---------------------------------------------------
+
+def spmv(op: int, m: int, n: int, row_ptr, col, val, x, alpha=1.0, beta=0.0, y=None, stream=None):
+    """CSRmv: y = alpha*op(A)*x + beta*y."""
+    torch = _torch()
+    if y is None:
+        y = torch.zeros(m if op == OP_N else n, dtype=torch.float32, device=x.device)
+    _check(lib().raptr_spmv(op, m, n, _ptr(row_ptr), _ptr(col), _ptr(val), alpha, _ptr(x), beta, _ptr(y),
+                            _stream(stream)))
+    return y
+
+
+def sensitivity(A: Matrix, stream=None):
+    """(FP64 column sums, FP32 image normalised to sum 1)."""
+    torch = _torch()
+    s64 = torch.empty(A.n, dtype=torch.float64, device=A.row_ptr.device)
+    s32 = torch.empty(A.n, dtype=torch.float32, device=A.row_ptr.device)
+    _check(lib().raptr_sensitivity(A.m, A.n, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(s64), _ptr(s32),
+                                   _stream(stream)))
+    return s64, s32
+
+
+def mlem_project(A: Matrix, y, x, c, ll=None, stream=None):
+    _check(lib().raptr_mlem_project(A.m, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(y), _ptr(x), _ptr(c),
+                                    _ptr(ll), _stream(stream)))
+
+
+def mlem_update(x, c, s, acc, stream=None):
+    _check(lib().raptr_mlem_update(x.numel(), _ptr(x), _ptr(c), _ptr(s), _ptr(acc), _stream(stream)))
+
+
+def divides(res, a, b, stream=None):
+    _check(lib().raptr_divides(_ptr(res), _ptr(a), _ptr(b), res.numel(), _stream(stream)))
+
+
+def divides_multiplies(res, a, b, c, stream=None):
+    _check(lib().raptr_divides_multiplies(_ptr(res), _ptr(a), _ptr(b), _ptr(c), res.numel(), _stream(stream)))
+
+
+def scales(x, alpha: float, stream=None):
+    _check(lib().raptr_scales(_ptr(x), alpha, x.numel(), _stream(stream)))
+
+
+def vsum(x, stream=None) -> float:
+    out = C.c_double()
+    _check(lib().raptr_sum(_ptr(x), x.numel(), C.byref(out), _stream(stream)))
+    return out.value
+
+
+def coo2csr(rows, m: int, stream=None):
+    torch = _torch()
+    rp = torch.empty(m + 1, dtype=torch.int64, device=rows.device)
+    _check(lib().raptr_coo2csr(_ptr(rows), rows.numel(), m, _ptr(rp), _stream(stream)))
+    return rp
+
+
+def csr2ecsr(yrow, csr, stream=None):
+    torch = _torch()
+    out = torch.empty(yrow.numel() + 1, dtype=torch.int64, device=csr.device)
+    _check(lib().raptr_csr2ecsr(_ptr(out), _ptr(yrow), yrow.numel(), _ptr(csr), csr.numel() - 1, _stream(stream)))
+    return out
+
+
+def reco_host(geom: Geometry, y: np.ndarray, nrays: int, seed: int, niter: int, sens: Optional[np.ndarray] = None,
+              x0: Optional[np.ndarray] = None, device: int = 0):
+    """The reco flow from host arrays: returns (x, stats dict)."""
+    gs = geom_struct(geom)
+    y = np.ascontiguousarray(y, np.float32)
+    assert y.size == geom.n_channels
+    x = np.zeros(geom.n_voxels, np.float32)
+    st = raptr_reco_stats()
+    sp = None if sens is None else np.ascontiguousarray(sens, np.float32)
+    xp = None if x0 is None else np.ascontiguousarray(x0, np.float32)
+    _check(lib().raptr_reco_host(C.byref(gs), device, y.ctypes.data, nrays, seed, niter,
+                                 None if sp is None else sp.ctypes.data, None if xp is None else xp.ctypes.data,
+                                 x.ctypes.data, C.byref(st)))
+    stats = {f: getattr(st, f) for f, _ in raptr_reco_stats._fields_}
+    return x, stats
+
+
+__all__ = [
+    "Geometry", "SMALL", "FULL", "FINE", "WORKLOADS", "epet_geometry", "phantom", "poisson_measurement", "Context",
+    "Matrix", "spmv", "sensitivity", "mlem_project", "mlem_update", "divides", "divides_multiplies", "scales",
+    "vsum", "coo2csr", "csr2ecsr", "reco_host", "lib", "RaptrError", "OP_N", "OP_T",
+]

@@ -1,0 +1,778 @@
+// The C ABI of raptr_b200 (include/raptr_b200.h): contexts, the chunked
+// system-matrix build, the candidate search, SpMV/MLEM entry points and the
+// end-to-end reconstruction from host buffers.
+//
+// Host code in this file computes the per-angle sine/cosine table with the
+// C library's sinf/cosf on the float expression of
+// src/MeasurementSetupTrafo2CartCoord.hpp:110-111; it is compiled with
+// -ffp-contract=off so the expression is evaluated as written.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+using namespace raptr;
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+
+namespace {
+
+thread_local std::string g_last_error;
+
+raptr_status fail(raptr_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+raptr_status cuda_fail(cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a sticky launch error for the next call
+  return fail(e == cudaErrorMemoryAllocation ? RAPTR_ERR_NOMEM : RAPTR_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define RCU(call)                                  \
+  do {                                             \
+    cudaError_t _e = (call);                       \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+
+#define RCHECK(expr)                              \
+  do {                                            \
+    raptr_status _s = (expr);                     \
+    if (_s != RAPTR_OK) return _s;                \
+  } while (0)
+
+// Makes `dev` current for the scope and restores the caller's device.
+struct DeviceScope {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceScope() {
+    int cur;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Per-angle (sin, cos) as the reference evaluates them:
+// sinf(T(M_PI)*ida*da/T(180.0)) with T = float, left to right.
+void sincos_table(const raptr_geom& g, std::vector<float2>& out) {
+  out.resize(size_t(g.na));
+  for (int a = 0; a < g.na; a++) {
+    float arg = float(M_PI) * float(a);
+    arg = arg * g.da;
+    arg = arg / 180.0f;
+    out[size_t(a)] = make_float2(sinf(arg), cosf(arg));
+  }
+}
+
+raptr_status validate_geom(const raptr_geom* g) {
+  if (!g) return fail(RAPTR_ERR_INVALID, "geometry is null");
+  for (int d = 0; d < 3; d++) {
+    if (g->grid_n[d] <= 0) return fail(RAPTR_ERR_INVALID, "grid_n must be positive");
+    if (!(g->grid_d[d] > 0.f) || !std::isfinite(g->grid_d[d])) return fail(RAPTR_ERR_INVALID, "grid_d must be positive");
+    if (!std::isfinite(g->grid_o[d])) return fail(RAPTR_ERR_INVALID, "grid_o must be finite");
+  }
+  if (g->grid_n[1] > 1024) return fail(RAPTR_ERR_UNSUPPORTED, "grid_n[1] above 1024 is not supported");
+  double nvox = double(g->grid_n[0]) * g->grid_n[1] * g->grid_n[2];
+  if (nvox >= 2147483647.0) return fail(RAPTR_ERR_UNSUPPORTED, "more than 2^31-1 voxels");
+  if (g->na <= 0 || g->n0z <= 0 || g->n0y <= 0 || g->n1z <= 0 || g->n1y <= 0)
+    return fail(RAPTR_ERR_INVALID, "detector counts must be positive");
+  double ncnl = double(g->na) * g->n0z * g->n0y * g->n1z * g->n1y;
+  if (ncnl >= 2147483647.0) return fail(RAPTR_ERR_UNSUPPORTED, "more than 2^31-1 channels");
+  if (!(g->segx > 0.f) || !(g->segy > 0.f) || !(g->segz > 0.f)) return fail(RAPTR_ERR_INVALID, "segment edges must be positive");
+  if (!std::isfinite(g->pos0x) || !std::isfinite(g->pos1x) || !std::isfinite(g->da))
+    return fail(RAPTR_ERR_INVALID, "setup positions and angle step must be finite");
+  return RAPTR_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context and matrix objects
+// ---------------------------------------------------------------------------
+
+struct raptr_ctx {
+  raptr_geom geom;
+  DGeom dg;
+  int device = 0;
+  float2* d_sincos = nullptr;
+  // Growable device scratch, carved per call.
+  unsigned char* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  // Small fixed device scratch.
+  int64_t* d_i64 = nullptr;   // 64 entries
+  int32_t* d_flags = nullptr; // 16 entries
+  double* d_f64 = nullptr;    // 64 entries
+
+  raptr_status ensure_scratch(size_t bytes) {
+    if (bytes <= scratch_bytes) return RAPTR_OK;
+    if (d_scratch) cudaFree(d_scratch);
+    d_scratch = nullptr;
+    scratch_bytes = 0;
+    size_t want = std::max(bytes, size_t(64) << 20);
+    RCU(cudaMalloc(&d_scratch, want));
+    scratch_bytes = want;
+    return RAPTR_OK;
+  }
+};
+
+struct raptr_matrix {
+  int device = 0;
+  int64_t m = 0, n = 0, nnz = 0, cap = 0;
+  int64_t* rp = nullptr;
+  int32_t* col = nullptr;
+  float* val = nullptr;
+};
+
+namespace {
+
+// Bump allocator over the context scratch.
+struct Carve {
+  unsigned char* base;
+  size_t off = 0;
+  explicit Carve(unsigned char* b) : base(b) {}
+  template <typename T>
+  T* take(size_t n) {
+    off = (off + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += n * sizeof(T);
+    return p;
+  }
+  static size_t need(std::initializer_list<size_t> bytes) {
+    size_t t = 0;
+    for (size_t b : bytes) t += ((b + 255) & ~size_t(255)) + 256;
+    return t;
+  }
+};
+
+constexpr size_t kStagingBudget = size_t(1) << 30;  // bytes of row staging per chunk
+
+// Output of a build: caller buffers (fixed capacity) or a library matrix
+// that grows.
+struct BuildOut {
+  int64_t* rp = nullptr;
+  int32_t* col = nullptr;
+  float* val = nullptr;
+  int64_t cap = 0;
+  raptr_matrix* grow = nullptr;  // non-null: grow this matrix on demand
+  int64_t n_list = 0;
+};
+
+raptr_status ensure_capacity(BuildOut& o, int64_t need, int64_t rows_done, cudaStream_t s) {
+  if (need <= o.cap || !o.grow) return RAPTR_OK;
+  double per_row = rows_done > 0 ? double(need) / double(rows_done) : 0.0;
+  int64_t projected = int64_t(per_row * double(o.n_list) * 1.05) + 1024;
+  int64_t ncap = std::max(need + (need >> 3), projected);
+  int32_t* ncol = nullptr;
+  float* nval = nullptr;
+  RCU(cudaMalloc(&ncol, size_t(ncap) * sizeof(int32_t)));
+  cudaError_t e = cudaMalloc(&nval, size_t(ncap) * sizeof(float));
+  if (e != cudaSuccess) {
+    cudaFree(ncol);
+    return cuda_fail(e, "cudaMalloc(matrix values)");
+  }
+  int64_t keep = std::min(o.cap, need);
+  if (o.col && keep > 0) {
+    RCU(cudaMemcpyAsync(ncol, o.col, size_t(keep) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    RCU(cudaMemcpyAsync(nval, o.val, size_t(keep) * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  }
+  RCU(cudaStreamSynchronize(s));
+  if (o.col) cudaFree(o.col);
+  if (o.val) cudaFree(o.val);
+  o.col = ncol;
+  o.val = nval;
+  o.cap = ncap;
+  o.grow->col = ncol;
+  o.grow->val = nval;
+  o.grow->cap = ncap;
+  return RAPTR_OK;
+}
+
+struct Builder {
+  raptr_ctx* ctx;
+  const int32_t* d_cnl;
+  int64_t n_list;
+  int nrays;
+  uint32_t seed;
+  const float* d_rays;
+  bool keep_zeros;
+  cudaStream_t s;
+  BuildOut& out;
+  int64_t total = 0;       // entries placed so far (host mirror of d_base)
+  int64_t rows_done = 0;
+
+  // Builds rows [row0, row0+nrows) at `level`, retrying at higher levels on
+  // table overflow, and places them.
+  raptr_status rows(int level, int64_t row0, int64_t nrows) {
+    const int H = sm_level_capacity(level);
+    int64_t per = std::max<int64_t>(1, int64_t(kStagingBudget / (size_t(H) * 8)));
+    per = std::min<int64_t>(per, 65536);
+    for (int64_t r = row0; r < row0 + nrows; r += per) {
+      const int64_t k = std::min(per, row0 + nrows - r);
+      size_t need = Carve::need({size_t(k) * H * sizeof(int32_t), size_t(k) * H * sizeof(float),
+                                 size_t(k) * sizeof(int32_t), size_t(k) * sizeof(int64_t),
+                                 size_t(scan_temp_elems(k)) * sizeof(int64_t)});
+      RCHECK(ctx->ensure_scratch(need));
+      Carve cv(ctx->d_scratch);
+      int32_t* st_col = cv.take<int32_t>(size_t(k) * H);
+      float* st_val = cv.take<float>(size_t(k) * H);
+      int32_t* row_nnz = cv.take<int32_t>(size_t(k));
+      int64_t* cand = cv.take<int64_t>(size_t(k));
+      (void)cand;
+      RCU(cudaMemsetAsync(ctx->d_flags, 0, sizeof(int32_t), s));
+      RCU(launch_sm_rows(level, ctx->dg, ctx->d_sincos, d_cnl, r, k, nrays, seed, d_rays, st_col, st_val, row_nnz,
+                         ctx->d_flags, s));
+      int32_t flags = 0;
+      RCU(cudaMemcpyAsync(&flags, ctx->d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      RCU(cudaStreamSynchronize(s));
+      if (flags & 4) return fail(RAPTR_ERR_INVALID, "a channel id is outside [0, number of channels)");
+      if (flags & 2) return fail(RAPTR_ERR_OVERFLOW, "ray walk did not terminate (internal error)");
+      if (flags & 1) {
+        if (level + 1 < sm_num_levels()) {
+          RCHECK(rows(level + 1, r, k));
+          continue;
+        }
+        return fail(RAPTR_ERR_OVERFLOW, "a row has more distinct voxels than the largest per-row table holds");
+      }
+      if (!keep_zeros) {
+        RCU(launch_rows_scan(row_nnz, k, out.rp + r, ctx->d_i64, s));
+      } else {
+        int64_t* counts = cand;
+        RCU(launch_wq_count(ctx->dg, ctx->d_sincos, d_cnl, r, k, 0, counts, ctx->d_flags, s));
+        RCU(launch_rows_scan_i64(counts, k, out.rp + r, ctx->d_i64, s));
+      }
+      int64_t new_total = 0;
+      RCU(cudaMemcpyAsync(&new_total, ctx->d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      RCU(cudaStreamSynchronize(s));
+      rows_done += k;
+      RCHECK(ensure_capacity(out, new_total, rows_done, s));
+      if (!keep_zeros) {
+        RCU(launch_rows_gather(st_col, st_val, H, out.rp + r, k, out.cap, out.col, out.val, s));
+      } else if (new_total <= out.cap) {
+        RCU(launch_wq_fill(ctx->dg, ctx->d_sincos, d_cnl, r, k, 0, out.rp + r, out.cap, nullptr, out.col, ctx->d_flags,
+                           s));
+        RCU(launch_expand_candidates(st_col, st_val, H, row_nnz, out.rp + r, k, out.col, out.val, s));
+      }
+      total = new_total;
+    }
+    return RAPTR_OK;
+  }
+};
+
+raptr_status run_build(raptr_ctx* ctx, const int32_t* d_cnl, int64_t n_list, int nrays, uint32_t seed,
+                       const float* d_rays, int32_t flags, BuildOut& out, int64_t* nnz_out, cudaStream_t s) {
+  if (n_list < 0) return fail(RAPTR_ERR_INVALID, "n_list must be non-negative");
+  if (n_list > 0 && !d_cnl) return fail(RAPTR_ERR_INVALID, "channel list is null");
+  if (nrays <= 0) return fail(RAPTR_ERR_INVALID, "nrays must be positive");
+  if (!out.rp) return fail(RAPTR_ERR_INVALID, "row pointer buffer is null");
+  RCU(cudaMemsetAsync(ctx->d_i64, 0, sizeof(int64_t), s));
+  RCU(cudaMemsetAsync(out.rp, 0, sizeof(int64_t), s));
+  out.n_list = n_list;
+  Builder b{ctx, d_cnl, n_list, nrays, seed, d_rays, (flags & RAPTR_SM_KEEP_ZEROS) != 0, s, out};
+  if (n_list > 0) RCHECK(b.rows(sm_pick_level(ctx->dg, nrays), 0, n_list));
+  RCU(cudaStreamSynchronize(s));
+  *nnz_out = b.total;
+  if (b.total > out.cap && !out.grow) {
+    return fail(RAPTR_ERR_CAPACITY, "matrix has " + std::to_string(b.total) + " entries, buffer holds " +
+                                        std::to_string(out.cap));
+  }
+  return RAPTR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int raptr_abi_version(void) { return RAPTR_ABI_VERSION; }
+
+const char* raptr_last_error(void) { return g_last_error.c_str(); }
+
+raptr_status raptr_ctx_create(const raptr_geom* geom, int device, raptr_ctx** out) {
+  if (!out) return fail(RAPTR_ERR_INVALID, "out is null");
+  *out = nullptr;
+  RCHECK(validate_geom(geom));
+  DeviceScope ds(device);
+  if (!ds.ok) return fail(RAPTR_ERR_CUDA, "cannot select device " + std::to_string(device));
+  raptr_ctx* c = new raptr_ctx;
+  c->geom = *geom;
+  c->dg = to_dgeom(*geom);
+  c->device = device;
+  std::vector<float2> tab;
+  sincos_table(*geom, tab);
+  cudaError_t e = cudaMalloc(&c->d_sincos, tab.size() * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_sincos, tab.data(), tab.size() * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_i64, 64 * sizeof(int64_t));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_flags, 16 * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_f64, 64 * sizeof(double));
+  if (e != cudaSuccess) {
+    raptr_ctx_destroy(c);
+    return cuda_fail(e, "context allocation");
+  }
+  *out = c;
+  return RAPTR_OK;
+}
+
+raptr_status raptr_ctx_destroy(raptr_ctx* ctx) {
+  if (!ctx) return RAPTR_OK;
+  DeviceScope ds(ctx->device);
+  cudaFree(ctx->d_sincos);
+  cudaFree(ctx->d_scratch);
+  cudaFree(ctx->d_i64);
+  cudaFree(ctx->d_flags);
+  cudaFree(ctx->d_f64);
+  delete ctx;
+  return RAPTR_OK;
+}
+
+int64_t raptr_ctx_num_channels(const raptr_ctx* ctx) {
+  if (!ctx) return 0;
+  const raptr_geom& g = ctx->geom;
+  return int64_t(g.na) * g.n0z * g.n0y * g.n1z * g.n1y;
+}
+
+int64_t raptr_ctx_num_voxels(const raptr_ctx* ctx) {
+  if (!ctx) return 0;
+  return int64_t(ctx->geom.grid_n[0]) * ctx->geom.grid_n[1] * ctx->geom.grid_n[2];
+}
+
+// ---- candidate search -------------------------------------------------------
+
+raptr_status raptr_candidate_counts(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int64_t* d_counts,
+                                    void* stream) {
+  if (!ctx || (n_list > 0 && (!d_cnl_ids || !d_counts))) return fail(RAPTR_ERR_INVALID, "null argument");
+  DeviceScope ds(ctx->device);
+  RCU(launch_wq_count(ctx->dg, ctx->d_sincos, d_cnl_ids, 0, n_list, 0, d_counts, nullptr, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_workqueue(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int64_t* list_id,
+                             int64_t* vxl_id, int64_t max_out, int32_t* d_cnl_out, int32_t* d_vxl_out,
+                             int64_t* n_found, void* stream) {
+  if (!ctx || !list_id || !vxl_id || !n_found) return fail(RAPTR_ERR_INVALID, "null argument");
+  *n_found = 0;
+  if (max_out <= 0) return RAPTR_OK;
+  if (!d_cnl_out || !d_vxl_out || (n_list > 0 && !d_cnl_ids)) return fail(RAPTR_ERR_INVALID, "null buffer");
+  const int64_t nvox = raptr_ctx_num_voxels(ctx);
+  if (*list_id < 0 || *vxl_id < 0 || *vxl_id >= nvox)
+    return fail(RAPTR_ERR_INVALID, "cursor out of range");  // the reference exits here (src/getWorkqueue.hpp:108-111)
+  DeviceScope ds(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  const int64_t kBatch = 16384;
+  int64_t li = *list_id, vi = *vxl_id, found = 0;
+  std::vector<int64_t> h_off;
+  while (li < n_list && found < max_out) {
+    const int64_t B = std::min(kBatch, n_list - li);
+    RCHECK(ctx->ensure_scratch(Carve::need({size_t(B) * 8, size_t(B + 1) * 8, size_t(scan_temp_elems(B)) * 8})));
+    Carve cv(ctx->d_scratch);
+    int64_t* counts = cv.take<int64_t>(size_t(B));
+    int64_t* offs = cv.take<int64_t>(size_t(B + 1));
+    int64_t* tmp = cv.take<int64_t>(size_t(scan_temp_elems(B)));
+    RCU(cudaMemsetAsync(ctx->d_flags, 0, sizeof(int32_t), s));
+    RCU(launch_wq_count(ctx->dg, ctx->d_sincos, d_cnl_ids, li, B, vi, counts, ctx->d_flags, s));
+    RCU(launch_scan_i64(counts, B, offs, tmp, s));
+    const int64_t remaining = max_out - found;
+    RCU(launch_wq_fill(ctx->dg, ctx->d_sincos, d_cnl_ids, li, B, vi, offs, remaining, d_cnl_out + found,
+                       d_vxl_out + found, nullptr, s));
+    h_off.resize(size_t(B + 1));
+    int32_t flags = 0;
+    RCU(cudaMemcpyAsync(h_off.data(), offs, size_t(B + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RCU(cudaMemcpyAsync(&flags, ctx->d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    RCU(cudaStreamSynchronize(s));
+    if (flags & 4) return fail(RAPTR_ERR_INVALID, "a channel id is outside [0, number of channels)");
+    const int64_t total = h_off[size_t(B)];
+    if (total >= remaining) {
+      // The last entry returned is entry `remaining-1` of this batch.
+      int64_t j = int64_t(std::upper_bound(h_off.begin(), h_off.end(), remaining - 1) - h_off.begin()) - 1;
+      int32_t last_v = 0;
+      RCU(cudaMemcpy(&last_v, d_vxl_out + found + remaining - 1, sizeof(int32_t), cudaMemcpyDeviceToHost));
+      found = max_out;
+      if (last_v < nvox - 1) {
+        *list_id = li + j;
+        *vxl_id = last_v + 1;
+      } else {
+        *list_id = li + j + 1;
+        *vxl_id = 0;
+      }
+      *n_found = found;
+      return RAPTR_OK;
+    }
+    found += total;
+    li += B;
+    vi = 0;
+  }
+  *list_id = n_list;
+  *vxl_id = 0;
+  *n_found = found;
+  return RAPTR_OK;
+}
+
+// ---- rays -----------------------------------------------------------------------
+
+raptr_status raptr_rays(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int32_t nrays, uint32_t seed,
+                        float* d_rays, void* stream) {
+  if (!ctx || nrays <= 0 || (n_list > 0 && (!d_cnl_ids || !d_rays))) return fail(RAPTR_ERR_INVALID, "bad argument");
+  DeviceScope ds(ctx->device);
+  RCU(launch_rays(ctx->dg, ctx->d_sincos, d_cnl_ids, n_list, nrays, seed, d_rays, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+// ---- system matrix ----------------------------------------------------------------
+
+raptr_status raptr_sm_build(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int32_t nrays, uint32_t seed,
+                            const float* d_rays, int32_t flags, int64_t capacity, int64_t* d_row_ptr, int32_t* d_col,
+                            float* d_val, int64_t* nnz_out, void* stream) {
+  if (!ctx || !nnz_out) return fail(RAPTR_ERR_INVALID, "null argument");
+  if (capacity < 0 || (capacity > 0 && (!d_col || !d_val))) return fail(RAPTR_ERR_INVALID, "bad output buffers");
+  DeviceScope ds(ctx->device);
+  BuildOut out;
+  out.rp = d_row_ptr;
+  out.col = d_col;
+  out.val = d_val;
+  out.cap = capacity;
+  return run_build(ctx, d_cnl_ids, n_list, nrays, seed, d_rays, flags, out, nnz_out, as_stream(stream));
+}
+
+raptr_status raptr_sm_build_alloc(raptr_ctx* ctx, const int32_t* d_cnl_ids, int64_t n_list, int32_t nrays,
+                                  uint32_t seed, const float* d_rays, int32_t flags, raptr_matrix** out_m,
+                                  void* stream) {
+  if (!ctx || !out_m) return fail(RAPTR_ERR_INVALID, "null argument");
+  *out_m = nullptr;
+  DeviceScope ds(ctx->device);
+  raptr_matrix* A = new raptr_matrix;
+  A->device = ctx->device;
+  A->m = n_list;
+  A->n = raptr_ctx_num_voxels(ctx);
+  cudaError_t e = cudaMalloc(&A->rp, size_t(n_list + 1) * sizeof(int64_t));
+  if (e != cudaSuccess) {
+    delete A;
+    return cuda_fail(e, "cudaMalloc(row pointers)");
+  }
+  BuildOut out;
+  out.rp = A->rp;
+  out.grow = A;
+  int64_t nnz = 0;
+  raptr_status st = run_build(ctx, d_cnl_ids, n_list, nrays, seed, d_rays, flags, out, &nnz, as_stream(stream));
+  if (st != RAPTR_OK) {
+    raptr_matrix_destroy(A);
+    return st;
+  }
+  A->nnz = nnz;
+  *out_m = A;
+  return RAPTR_OK;
+}
+
+raptr_status raptr_matrix_info(const raptr_matrix* A, int64_t* m, int64_t* n, int64_t* nnz, int64_t** d_row_ptr,
+                               int32_t** d_col, float** d_val) {
+  if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
+  if (m) *m = A->m;
+  if (n) *n = A->n;
+  if (nnz) *nnz = A->nnz;
+  if (d_row_ptr) *d_row_ptr = A->rp;
+  if (d_col) *d_col = A->col;
+  if (d_val) *d_val = A->val;
+  return RAPTR_OK;
+}
+
+raptr_status raptr_matrix_destroy(raptr_matrix* A) {
+  if (!A) return RAPTR_OK;
+  DeviceScope ds(A->device);
+  cudaFree(A->rp);
+  cudaFree(A->col);
+  cudaFree(A->val);
+  delete A;
+  return RAPTR_OK;
+}
+
+// ---- sparse formats ---------------------------------------------------------------
+
+raptr_status raptr_coo2csr(const int32_t* d_rows, int64_t nnz, int64_t m, int64_t* d_row_ptr, void* stream) {
+  if (m < 0 || nnz < 0 || !d_row_ptr || (nnz > 0 && !d_rows)) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_coo2csr(d_rows, nnz, m, d_row_ptr, nullptr, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_csr2ecsr(int64_t* d_ecsr, const int32_t* d_yrow, int64_t nnzr, const int64_t* d_csr, int64_t m,
+                            void* stream) {
+  if (nnzr < 0 || m < 0 || !d_ecsr || !d_csr || (nnzr > 0 && !d_yrow)) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_csr2ecsr(d_ecsr, d_yrow, nnzr, d_csr, m, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+// ---- SpMV -----------------------------------------------------------------------------
+
+raptr_status raptr_spmv(int32_t op, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                        const float* d_val, float alpha, const float* d_x, float beta, float* d_y, void* stream) {
+  if (op != RAPTR_OP_N && op != RAPTR_OP_T) return fail(RAPTR_ERR_INVALID, "op must be RAPTR_OP_N or RAPTR_OP_T");
+  if (m < 0 || n < 0 || !d_row_ptr || !d_x || !d_y) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_spmv(op, m, n, d_row_ptr, d_col, d_val, alpha, d_x, beta, d_y, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+// ---- element-wise ---------------------------------------------------------------------
+
+raptr_status raptr_divides(float* d_res, const float* d_dividend, const float* d_divisor, int64_t n, void* stream) {
+  if (n < 0 || (n > 0 && (!d_res || !d_dividend || !d_divisor))) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_divides(d_res, d_dividend, d_divisor, n, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_divides_multiplies(float* d_res, const float* d_a, const float* d_b, const float* d_c, int64_t n,
+                                      void* stream) {
+  if (n < 0 || (n > 0 && (!d_res || !d_a || !d_b || !d_c))) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_divides_multiplies(d_res, d_a, d_b, d_c, n, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_scales(float* d_x, float alpha, int64_t n, void* stream) {
+  if (n < 0 || (n > 0 && !d_x)) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_scales(d_x, alpha, n, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_sum(const float* d_x, int64_t n, double* sum_out, void* stream) {
+  if (n < 0 || !sum_out || (n > 0 && !d_x)) return fail(RAPTR_ERR_INVALID, "bad argument");
+  cudaStream_t s = as_stream(stream);
+  double* acc = nullptr;
+  RCU(cudaMallocAsync(&acc, sizeof(double), s));
+  cudaError_t e = launch_sum(d_x, n, acc, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sum_out, acc, sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(acc, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "raptr_sum");
+  return RAPTR_OK;
+}
+
+// ---- sensitivity and MLEM -------------------------------------------------------------
+
+raptr_status raptr_sensitivity(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                               const float* d_val, double* d_s64, float* d_s32, void* stream) {
+  if (m < 0 || n <= 0 || !d_row_ptr || !d_s64) return fail(RAPTR_ERR_INVALID, "bad argument");
+  cudaStream_t s = as_stream(stream);
+  RCU(cudaMemsetAsync(d_s64, 0, size_t(n) * sizeof(double), s));
+  RCU(launch_column_sums(m, d_row_ptr, d_col, d_val, d_s64, s));
+  if (d_s32) {
+    double* acc = nullptr;
+    RCU(cudaMallocAsync(&acc, sizeof(double), s));
+    cudaError_t e = launch_sum_f64(d_s64, n, acc, s);
+    if (e == cudaSuccess) e = launch_sens_normalise(n, d_s64, acc, d_s32, s);
+    cudaFreeAsync(acc, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sensitivity normalisation");
+  }
+  return RAPTR_OK;
+}
+
+raptr_status raptr_mlem_project(int64_t m, const int64_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                                const float* d_y, const float* d_x, float* d_c, double* d_ll, void* stream) {
+  if (m < 0 || !d_row_ptr || !d_y || !d_x || !d_c) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_mlem_project(m, d_row_ptr, d_col, d_val, d_y, d_x, d_c, d_ll, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_mlem_update(int64_t n, float* d_x, float* d_c, const float* d_s, double* d_acc, void* stream) {
+  if (n <= 0 || !d_x || !d_c || !d_s || !d_acc) return fail(RAPTR_ERR_INVALID, "bad argument");
+  cudaStream_t s = as_stream(stream);
+  RCU(cudaMemsetAsync(d_acc, 0, sizeof(double), s));
+  RCU(launch_mlem_update(n, d_x, d_c, d_s, d_acc, s));
+  RCU(launch_mlem_normalise(n, d_x, d_c, d_acc, s));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                        const float* d_val, const float* d_y, const float* d_s, float* d_x, int32_t n_iter,
+                        const raptr_mlem_opts* opts, void* stream) {
+  if (!ctx || m < 0 || n <= 0 || n_iter < 0 || !d_row_ptr || !d_y || !d_s || !d_x)
+    return fail(RAPTR_ERR_INVALID, "bad argument");
+  if (n_iter == 0) return RAPTR_OK;
+  DeviceScope ds(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  const bool want_ll = opts && opts->h_loglik;
+  const bool use_graph = opts && opts->use_graph;
+  RCHECK(ctx->ensure_scratch(Carve::need({size_t(n) * sizeof(float), size_t(2 * n_iter + 2) * sizeof(double)})));
+  Carve cv(ctx->d_scratch);
+  float* c = cv.take<float>(size_t(n));
+  double* acc = cv.take<double>(size_t(2 * n_iter + 2));
+  double* ll = acc + 2;
+  RCU(cudaMemsetAsync(c, 0, size_t(n) * sizeof(float), s));
+  RCU(cudaMemsetAsync(acc, 0, size_t(2 * n_iter + 2) * sizeof(double), s));
+
+  auto enqueue = [&](cudaStream_t q) -> cudaError_t {
+    for (int32_t it = 0; it < n_iter; it++) {
+      cudaError_t e = launch_mlem_project(m, d_row_ptr, d_col, d_val, d_y, d_x, c, want_ll ? ll + 2 * it : nullptr, q);
+      if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, sizeof(double), q);
+      if (e == cudaSuccess) e = launch_mlem_update(n, d_x, c, d_s, acc, q);
+      if (e == cudaSuccess) e = launch_mlem_normalise(n, d_x, c, acc, q);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+
+  if (!use_graph) {
+    RCU(enqueue(s));
+  } else {
+    cudaStream_t cap;
+    RCU(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaEvent_t ev;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cap, ev, 0);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      cudaError_t e1 = enqueue(cap);
+      cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+      e = (e1 != cudaSuccess) ? e1 : e2;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, cap);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, cap);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cap);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaEventDestroy(ev);
+    cudaStreamDestroy(cap);
+    if (e != cudaSuccess) return cuda_fail(e, "MLEM graph");
+  }
+  if (want_ll) {
+    std::vector<double> h(size_t(2 * n_iter));
+    RCU(cudaMemcpyAsync(h.data(), ll, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    double ysum = 0.0;
+    RCU(launch_sum(d_y, m, acc + 1, s));
+    RCU(cudaMemcpyAsync(&ysum, acc + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+    RCU(cudaStreamSynchronize(s));
+    // Poisson log-likelihood (without the log y! term) at the best global
+    // scale of A x: sum y log(k Ax) - k sum Ax with k = sum y / sum Ax.
+    for (int32_t it = 0; it < n_iter; it++) {
+      double s1 = h[size_t(2 * it)], s2 = h[size_t(2 * it + 1)];
+      opts->h_loglik[it] = s1 + ysum * std::log(ysum / s2) - ysum;
+    }
+  }
+  return RAPTR_OK;
+}
+
+// ---- end-to-end -----------------------------------------------------------------------
+
+raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_y, int32_t nrays, uint32_t seed,
+                             int32_t n_iter, const float* h_sens, const float* h_x0, float* h_x,
+                             raptr_reco_stats* stats) {
+  if (!h_y || !h_x || nrays <= 0 || n_iter < 0) return fail(RAPTR_ERR_INVALID, "bad argument");
+  raptr_ctx* ctx = nullptr;
+  RCHECK(raptr_ctx_create(geom, device, &ctx));
+  DeviceScope ds(device);
+  const int64_t M = raptr_ctx_num_channels(ctx), N = raptr_ctx_num_voxels(ctx);
+  cudaStream_t s;
+  RCU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaEvent_t ev[5];
+  for (auto& e : ev) cudaEventCreate(&e);
+  raptr_matrix* A = nullptr;
+  float *d_y = nullptr, *d_x = nullptr, *d_s = nullptr;
+  int32_t* d_list = nullptr;
+  double* d_s64 = nullptr;
+  raptr_status st = RAPTR_OK;
+  auto cleanup = [&]() {
+    raptr_matrix_destroy(A);
+    cudaFree(d_y);
+    cudaFree(d_x);
+    cudaFree(d_s);
+    cudaFree(d_list);
+    cudaFree(d_s64);
+    for (auto& e : ev) cudaEventDestroy(e);
+    cudaStreamDestroy(s);
+    raptr_ctx_destroy(ctx);
+  };
+#define RSTEP(expr)                                         \
+  do {                                                      \
+    cudaError_t _e = (expr);                                \
+    if (_e != cudaSuccess) {                                \
+      st = cuda_fail(_e, #expr);                            \
+      cleanup();                                            \
+      return st;                                            \
+    }                                                       \
+  } while (0)
+  RSTEP(cudaEventRecord(ev[0], s));
+  RSTEP(cudaMalloc(&d_y, size_t(M) * sizeof(float)));
+  RSTEP(cudaMalloc(&d_x, size_t(N) * sizeof(float)));
+  RSTEP(cudaMalloc(&d_s, size_t(N) * sizeof(float)));
+  RSTEP(cudaMalloc(&d_list, size_t(M) * sizeof(int32_t)));
+  RSTEP(cudaMemcpyAsync(d_y, h_y, size_t(M) * sizeof(float), cudaMemcpyHostToDevice, s));
+  int64_t h2d = M * int64_t(sizeof(float));
+  RSTEP(launch_iota(d_list, M, s));
+  RSTEP(cudaEventRecord(ev[1], s));
+  st = raptr_sm_build_alloc(ctx, d_list, M, nrays, seed, nullptr, 0, &A, s);
+  if (st != RAPTR_OK) {
+    std::string msg = g_last_error;
+    cleanup();
+    return fail(st, msg);
+  }
+  RSTEP(cudaEventRecord(ev[2], s));
+  if (!h_sens) {
+    RSTEP(cudaMalloc(&d_s64, size_t(N) * sizeof(double)));
+    st = raptr_sensitivity(A->m, N, A->rp, A->col, A->val, d_s64, d_s, s);
+  } else {
+    RSTEP(cudaMemcpyAsync(d_s, h_sens, size_t(N) * sizeof(float), cudaMemcpyHostToDevice, s));
+    h2d += N * int64_t(sizeof(float));
+    // s /= sum(s) as src/tests/reco.cu:202-204
+    RSTEP(launch_sum(d_s, N, ctx->d_f64, s));
+    double sum = 0.0;
+    RSTEP(cudaMemcpyAsync(&sum, ctx->d_f64, sizeof(double), cudaMemcpyDeviceToHost, s));
+    RSTEP(cudaStreamSynchronize(s));
+    RSTEP(launch_scales(d_s, float(1. / float(sum)), N, s));
+  }
+  if (st != RAPTR_OK) {
+    std::string msg = g_last_error;
+    cleanup();
+    return fail(st, msg);
+  }
+  if (h_x0) {
+    RSTEP(cudaMemcpyAsync(d_x, h_x0, size_t(N) * sizeof(float), cudaMemcpyHostToDevice, s));
+    h2d += N * int64_t(sizeof(float));
+  } else {
+    // Uniform image normalised to sum 1 (src/tests/reco.cu:145-158).
+    std::vector<float> ones(size_t(N), float(1. / float(N)));
+    RSTEP(cudaMemcpyAsync(d_x, ones.data(), size_t(N) * sizeof(float), cudaMemcpyHostToDevice, s));
+    RSTEP(cudaStreamSynchronize(s));
+    h2d += N * int64_t(sizeof(float));
+  }
+  RSTEP(cudaEventRecord(ev[3], s));
+  raptr_mlem_opts o{1, nullptr};
+  st = raptr_mlem(ctx, A->m, N, A->rp, A->col, A->val, d_y, d_s, d_x, n_iter, &o, s);
+  if (st != RAPTR_OK) {
+    std::string msg = g_last_error;
+    cleanup();
+    return fail(st, msg);
+  }
+  RSTEP(cudaEventRecord(ev[4], s));
+  RSTEP(cudaMemcpyAsync(h_x, d_x, size_t(N) * sizeof(float), cudaMemcpyDeviceToHost, s));
+  RSTEP(cudaStreamSynchronize(s));
+  if (stats) {
+    float t;
+    cudaEventElapsedTime(&t, ev[1], ev[2]);
+    stats->build_ms = t;
+    cudaEventElapsedTime(&t, ev[2], ev[3]);
+    stats->sens_ms = t;
+    cudaEventElapsedTime(&t, ev[3], ev[4]);
+    stats->iter_ms = t;
+    cudaEventElapsedTime(&t, ev[0], ev[4]);
+    stats->total_ms = t;
+    stats->nnz = A->nnz;
+    stats->h2d_bytes = h2d;
+    stats->d2h_bytes = N * int64_t(sizeof(float));
+  }
+#undef RSTEP
+  cleanup();
+  return RAPTR_OK;
+}
+
+}  // extern "C"

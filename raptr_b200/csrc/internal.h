@@ -1,0 +1,98 @@
+// Internal interface between the C ABI (api.cu) and the kernel translation
+// units.  Host launch wrappers only; no device code here.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace raptr {
+
+// ---- system matrix rows (kernels_sm.cu) ----------------------------------
+
+// Hash/slot capacity levels for the per-channel accumulation table; a row
+// whose distinct voxels do not fit is re-run at the next level.
+int sm_num_levels();
+int sm_level_capacity(int level);   // entries per row slot
+int sm_level_threads(int level);
+int sm_pick_level(const DGeom& g, int nrays);
+
+// Builds rows [row0, row0+nrows) of the list into staging slots (slot i at
+// st_col/st_val + i*capacity).  row_nnz[i] = entries, or -1 if the table
+// overflowed.  *d_flags |= 1 on overflow, |= 4 for a channel id out of range.
+cudaError_t launch_sm_rows(int level, const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0,
+                           int64_t nrows, int nrays, uint32_t seed, const float* d_rays, int32_t* st_col,
+                           float* st_val, int32_t* row_nnz, int32_t* d_flags, cudaStream_t s);
+
+// Exclusive scan of row_nnz[0..n) into row_ptr[0..n] (int64) starting at
+// *d_base; *d_base is advanced by the sum.  One block.
+cudaError_t launch_rows_scan(const int32_t* row_nnz, int64_t n, int64_t* row_ptr, int64_t* d_base, cudaStream_t s);
+
+cudaError_t launch_rows_scan_i64(const int64_t* counts, int64_t n, int64_t* row_ptr, int64_t* d_base, cudaStream_t s);
+
+// Copies staged rows to their final CSR position; entries at or beyond
+// `capacity` are not written.
+cudaError_t launch_rows_gather(const int32_t* st_col, const float* st_val, int slot_cap, const int64_t* row_ptr,
+                               int64_t nrows, int64_t capacity, int32_t* col, float* val, cudaStream_t s);
+
+// Keep-zeros expansion of one row block: for every candidate of the row
+// (written in order by the workqueue fill), look up its value in the
+// zero-free staged row.
+cudaError_t launch_expand_candidates(const int32_t* st_col, const float* st_val, int slot_cap, const int32_t* row_nnz,
+                                     const int64_t* cand_ptr, int64_t nrows, int32_t* cand_vxl, float* out_val,
+                                     cudaStream_t s);
+
+cudaError_t launch_rays(const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t n, int nrays,
+                        uint32_t seed, float* d_rays, cudaStream_t s);
+
+// ---- candidate search (kernels_sm.cu) --------------------------------------
+
+// counts[i] = candidates of list entry li0+i; entry li0 starts at voxel
+// start_vxl.  A channel id out of range counts 0 and sets *d_flags |= 4.
+cudaError_t launch_wq_count(const DGeom& g, const float2* d_sincos, const int32_t* d_list, int64_t li0, int64_t n,
+                            int64_t start_vxl, int64_t* d_counts, int32_t* d_flags, cudaStream_t s);
+// Writes candidate k of list entry li0+i to position offsets[i]+k when below
+// max_out (d_cnl_out may be null).
+cudaError_t launch_wq_fill(const DGeom& g, const float2* d_sincos, const int32_t* d_list, int64_t li0, int64_t n,
+                           int64_t start_vxl, const int64_t* d_offsets, int64_t max_out, int32_t* d_cnl_out,
+                           int32_t* d_vxl_out, int32_t* d_flags, cudaStream_t s);
+
+// ---- scans and small utilities (kernels_util.cu) ---------------------------
+
+// Exclusive scan of int64 counts into offsets (n+1 entries, offsets[n] = total).
+// temp must hold scan_temp_elems(n) int64.
+int64_t scan_temp_elems(int64_t n);
+cudaError_t launch_scan_i64(const int64_t* in, int64_t n, int64_t* out, int64_t* temp, cudaStream_t s);
+
+cudaError_t launch_coo2csr(const int32_t* rows, int64_t nnz, int64_t m, int64_t* row_ptr, int64_t* temp,
+                           cudaStream_t s);
+cudaError_t launch_csr2ecsr(int64_t* ecsr, const int32_t* yrow, int64_t nnzr, const int64_t* csr, int64_t m,
+                            cudaStream_t s);
+
+// ---- SpMV and MLEM (kernels_mlem.cu) ---------------------------------------
+
+cudaError_t launch_spmv(int op, int64_t m, int64_t n, const int64_t* rp, const int32_t* col, const float* val,
+                        float alpha, const float* x, float beta, float* y, cudaStream_t s);
+cudaError_t launch_divides(float* r, const float* a, const float* b, int64_t n, cudaStream_t s);
+cudaError_t launch_divides_multiplies(float* r, const float* a, const float* b, const float* c, int64_t n,
+                                      cudaStream_t s);
+cudaError_t launch_scales(float* x, float alpha, int64_t n, cudaStream_t s);
+cudaError_t launch_sum(const float* x, int64_t n, double* d_acc, cudaStream_t s);
+cudaError_t launch_column_sums(int64_t m, const int64_t* rp, const int32_t* col, const float* val, double* s64,
+                               cudaStream_t s);
+cudaError_t launch_sens_normalise(int64_t n, const double* s64, const double* d_total, float* s32, cudaStream_t s);
+cudaError_t launch_sum_f64(const double* x, int64_t n, double* d_acc, cudaStream_t s);
+
+// c += A^T (y / (A x)); when d_ll is non-null, d_ll[0] += sum y*log(Ax),
+// d_ll[1] += sum Ax (FP64).
+cudaError_t launch_mlem_project(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const float* y,
+                                const float* x, float* c, double* d_ll, cudaStream_t s);
+// x = x*c/(s + (s==0)); d_acc[0] += sum(x) (FP64).
+cudaError_t launch_mlem_update(int64_t n, float* x, const float* c, const float* sens, double* d_acc, cudaStream_t s);
+// x *= float(1/float(d_acc[0])); c = 0; d_acc[0] reset by the next project.
+cudaError_t launch_mlem_normalise(int64_t n, float* x, float* c, double* d_acc, cudaStream_t s);
+cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s);
+cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s);
+
+}  // namespace raptr

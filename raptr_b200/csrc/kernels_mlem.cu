@@ -1,0 +1,352 @@
+// CSR SpMV (forward and back projection), the MLEM element-wise operations
+// and the fused MLEM projection for sm_100a.
+//
+// All kernels here are HBM-bandwidth bound: the matrix streams once per
+// call with 16-byte vector loads (four columns + four values per lane), the
+// image x (a few MB) stays in L2, and back projection accumulates with
+// fire-and-forget float reductions (red.global.add.f32) into the image,
+// which is also L2-resident.
+#include <cstdint>
+
+#include "internal.h"
+
+namespace raptr {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block reduction of a double into *dst (one atomic per block).
+__device__ __forceinline__ void block_add_double(double v, double* dst) {
+  __shared__ double ws[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sum_d(v);
+  if (lane == 0) ws[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double w = (lane < int(blockDim.x >> 5)) ? ws[lane] : 0.0;
+    w = warp_sum_d(w);
+    if (lane == 0 && w != 0.0) atomicAdd(dst, w);
+  }
+}
+
+// Dot product of CSR row [b, e) with x, computed by one warp; every lane
+// returns the sum.  Head and tail are scalar, the aligned body uses
+// 16-byte loads of four columns and four values per lane.
+template <bool VEC>
+__device__ __forceinline__ float row_dot(const int32_t* __restrict__ col, const float* __restrict__ val, int64_t b,
+                                         int64_t e, const float* __restrict__ x, int lane) {
+  float acc = 0.f;
+  if (!VEC) {
+    for (int64_t k = b + lane; k < e; k += 32) acc += __ldg(val + k) * __ldg(x + __ldg(col + k));
+    return warp_sum(acc);
+  }
+  int64_t a = (b + 3) & ~int64_t(3);
+  if (a > e) a = e;
+  if (b + lane < a) acc += __ldg(val + b + lane) * __ldg(x + __ldg(col + b + lane));
+  const int64_t nq = (e - a) >> 2;
+  const int4* c4 = reinterpret_cast<const int4*>(col + a);
+  const float4* v4 = reinterpret_cast<const float4*>(val + a);
+  int64_t q = lane;
+  for (; q + 32 < nq; q += 64) {
+    int4 c0 = __ldg(c4 + q);
+    float4 w0 = __ldg(v4 + q);
+    int4 c1 = __ldg(c4 + q + 32);
+    float4 w1 = __ldg(v4 + q + 32);
+    acc += w0.x * __ldg(x + c0.x) + w0.y * __ldg(x + c0.y) + w0.z * __ldg(x + c0.z) + w0.w * __ldg(x + c0.w);
+    acc += w1.x * __ldg(x + c1.x) + w1.y * __ldg(x + c1.y) + w1.z * __ldg(x + c1.z) + w1.w * __ldg(x + c1.w);
+  }
+  if (q < nq) {
+    int4 c0 = __ldg(c4 + q);
+    float4 w0 = __ldg(v4 + q);
+    acc += w0.x * __ldg(x + c0.x) + w0.y * __ldg(x + c0.y) + w0.z * __ldg(x + c0.z) + w0.w * __ldg(x + c0.w);
+  }
+  const int64_t t = a + (nq << 2) + lane;
+  if (t < e) acc += __ldg(val + t) * __ldg(x + __ldg(col + t));
+  return warp_sum(acc);
+}
+
+// y[col] += f * val over CSR row [b, e), by one warp.  Streaming loads:
+// this is the last use of the row in the pass.
+template <bool VEC>
+__device__ __forceinline__ void row_scatter(const int32_t* __restrict__ col, const float* __restrict__ val, int64_t b,
+                                            int64_t e, float f, float* __restrict__ y, int lane) {
+  if (!VEC) {
+    for (int64_t k = b + lane; k < e; k += 32) atomicAdd(y + __ldcs(col + k), __ldcs(val + k) * f);
+    return;
+  }
+  int64_t a = (b + 3) & ~int64_t(3);
+  if (a > e) a = e;
+  if (b + lane < a) atomicAdd(y + __ldcs(col + b + lane), __ldcs(val + b + lane) * f);
+  const int64_t nq = (e - a) >> 2;
+  const int4* c4 = reinterpret_cast<const int4*>(col + a);
+  const float4* v4 = reinterpret_cast<const float4*>(val + a);
+  for (int64_t q = lane; q < nq; q += 32) {
+    int4 c = __ldcs(c4 + q);
+    float4 w = __ldcs(v4 + q);
+    atomicAdd(y + c.x, w.x * f);
+    atomicAdd(y + c.y, w.y * f);
+    atomicAdd(y + c.z, w.z * f);
+    atomicAdd(y + c.w, w.w * f);
+  }
+  const int64_t t = a + (nq << 2) + lane;
+  if (t < e) atomicAdd(y + __ldcs(col + t), __ldcs(val + t) * f);
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads) spmv_n_kernel(int64_t m, const int64_t* __restrict__ rp,
+                                                          const int32_t* __restrict__ col,
+                                                          const float* __restrict__ val, float alpha,
+                                                          const float* __restrict__ x, float beta,
+                                                          float* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+    float d = row_dot<VEC>(col, val, rp[r], rp[r + 1], x, lane);
+    if (lane == 0) y[r] = (beta == 0.f) ? alpha * d : alpha * d + beta * y[r];
+  }
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads) spmv_t_kernel(int64_t m, const int64_t* __restrict__ rp,
+                                                          const int32_t* __restrict__ col,
+                                                          const float* __restrict__ val, float alpha,
+                                                          const float* __restrict__ x, float* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+    float f = alpha * x[r];
+    if (f != 0.f) row_scatter<VEC>(col, val, rp[r], rp[r + 1], f, y, lane);
+  }
+}
+
+__global__ void scale_kernel(float* __restrict__ y, float beta, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    y[i] = (beta == 0.f) ? 0.f : beta * y[i];
+}
+
+__global__ void divides_kernel(float* __restrict__ r, const float* __restrict__ a, const float* __restrict__ b,
+                               int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    r[i] = a[i] / b[i];
+}
+
+// result = a * b / (c + (c == 0)) (src/mlemOperations.hpp:61-76).
+__global__ void divmul_kernel(float* __restrict__ r, const float* __restrict__ a, const float* __restrict__ b,
+                              const float* __restrict__ c, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    float dvs = c[i];
+    dvs += float(dvs == 0.f);
+    r[i] = __fdiv_rn(__fmul_rn(a[i], b[i]), dvs);
+  }
+}
+
+__global__ void scales_kernel(float* __restrict__ x, float alpha, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    x[i] = __fmul_rn(alpha, x[i]);
+}
+
+__global__ void __launch_bounds__(kThreads) sum_kernel(const float* __restrict__ x, int64_t n, double* acc) {
+  double s = 0.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    s += double(x[i]);
+  block_add_double(s, acc);
+}
+
+__global__ void __launch_bounds__(kThreads) sum_f64_kernel(const double* __restrict__ x, int64_t n, double* acc) {
+  double s = 0.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    s += x[i];
+  block_add_double(s, acc);
+}
+
+__global__ void __launch_bounds__(kThreads) colsum_kernel(int64_t m, const int64_t* __restrict__ rp,
+                                                          const int32_t* __restrict__ col,
+                                                          const float* __restrict__ val, double* __restrict__ s) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+    const int64_t b = rp[r], e = rp[r + 1];
+    for (int64_t k = b + lane; k < e; k += 32) atomicAdd(s + __ldcs(col + k), double(__ldcs(val + k)));
+  }
+}
+
+__global__ void sens_norm_kernel(int64_t n, const double* __restrict__ s64, const double* __restrict__ total,
+                                 float* __restrict__ s32) {
+  const double t = *total;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    s32[i] = float(s64[i] / t);
+}
+
+// Fused MLEM projection: per measured row, yt = <a_i, x>, e = y_i / yt
+// (no zero guard, src/mlemOperations.hpp:44-54), c += e * a_i.  A row with
+// y_i == 0 is not part of the measurement (the reference's matrix has no row
+// for it) and is skipped.
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads) mlem_project_kernel(int64_t m, const int64_t* __restrict__ rp,
+                                                                const int32_t* __restrict__ col,
+                                                                const float* __restrict__ val,
+                                                                const float* __restrict__ y,
+                                                                const float* __restrict__ x, float* __restrict__ c,
+                                                                double* __restrict__ ll) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  double ly = 0.0, lt = 0.0;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+    const float yi = __ldg(y + r);
+    if (yi == 0.f) continue;
+    const int64_t b = rp[r], e = rp[r + 1];
+    const float yt = row_dot<VEC>(col, val, b, e, x, lane);
+    const float f = __fdiv_rn(yi, yt);
+    if (ll && lane == 0) {
+      ly += double(yi) * log(double(yt));
+      lt += double(yt);
+    }
+    row_scatter<VEC>(col, val, b, e, f, c, lane);
+  }
+  if (ll) {
+    block_add_double(ly, ll);
+    __syncthreads();
+    block_add_double(lt, ll + 1);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) mlem_update_kernel(int64_t n, float* __restrict__ x,
+                                                               const float* __restrict__ c,
+                                                               const float* __restrict__ s, double* __restrict__ acc) {
+  double sum = 0.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    float dvs = s[i];
+    dvs += float(dvs == 0.f);
+    float xx = __fdiv_rn(__fmul_rn(x[i], c[i]), dvs);
+    x[i] = xx;
+    sum += double(xx);
+  }
+  block_add_double(sum, acc);
+}
+
+__global__ void mlem_normalise_kernel(int64_t n, float* __restrict__ x, float* __restrict__ c,
+                                      const double* __restrict__ acc) {
+  const float norm = float(*acc);
+  const float scale = float(1.0 / double(norm));
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    x[i] = __fmul_rn(scale, x[i]);
+    c[i] = 0.f;
+  }
+}
+
+// The 16-byte vector path needs 16-byte aligned column and value arrays.
+bool aligned16(const void* a, const void* b) {
+  return ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15u) == 0;
+}
+
+unsigned ew_grid(int64_t n) {
+  int64_t b = (n + kThreads - 1) / kThreads;
+  if (b < 1) b = 1;
+  if (b > 148 * 8) b = 148 * 8;
+  return unsigned(b);
+}
+
+unsigned row_grid(int64_t m) {
+  int64_t b = (m * 32 + kThreads - 1) / kThreads;
+  if (b < 1) b = 1;
+  if (b > 148 * 16) b = 148 * 16;
+  return unsigned(b);
+}
+
+}  // namespace
+
+cudaError_t launch_spmv(int op, int64_t m, int64_t n, const int64_t* rp, const int32_t* col, const float* val,
+                        float alpha, const float* x, float beta, float* y, cudaStream_t s) {
+  if (op == RAPTR_OP_N) {
+    if (m > 0) {
+      if (aligned16(col, val)) spmv_n_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, beta, y);
+      else spmv_n_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, beta, y);
+    }
+  } else {
+    if (beta != 1.f && n > 0) scale_kernel<<<ew_grid(n), kThreads, 0, s>>>(y, beta, n);
+    if (m > 0) {
+      if (aligned16(col, val)) spmv_t_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, y);
+      else spmv_t_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, y);
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_divides(float* r, const float* a, const float* b, int64_t n, cudaStream_t s) {
+  if (n > 0) divides_kernel<<<ew_grid(n), kThreads, 0, s>>>(r, a, b, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_divides_multiplies(float* r, const float* a, const float* b, const float* c, int64_t n,
+                                      cudaStream_t s) {
+  if (n > 0) divmul_kernel<<<ew_grid(n), kThreads, 0, s>>>(r, a, b, c, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scales(float* x, float alpha, int64_t n, cudaStream_t s) {
+  if (n > 0) scales_kernel<<<ew_grid(n), kThreads, 0, s>>>(x, alpha, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sum(const float* x, int64_t n, double* d_acc, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_acc, 0, sizeof(double), s);
+  if (e != cudaSuccess) return e;
+  if (n > 0) sum_kernel<<<ew_grid(n), kThreads, 0, s>>>(x, n, d_acc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sum_f64(const double* x, int64_t n, double* d_acc, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_acc, 0, sizeof(double), s);
+  if (e != cudaSuccess) return e;
+  if (n > 0) sum_f64_kernel<<<ew_grid(n), kThreads, 0, s>>>(x, n, d_acc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_column_sums(int64_t m, const int64_t* rp, const int32_t* col, const float* val, double* s64,
+                               cudaStream_t s) {
+  if (m > 0) colsum_kernel<<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, s64);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sens_normalise(int64_t n, const double* s64, const double* d_total, float* s32, cudaStream_t s) {
+  if (n > 0) sens_norm_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, s64, d_total, s32);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlem_project(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const float* y,
+                                const float* x, float* c, double* d_ll, cudaStream_t s) {
+  if (m > 0) {
+    if (aligned16(col, val)) mlem_project_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, c, d_ll);
+    else mlem_project_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, c, d_ll);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlem_update(int64_t n, float* x, const float* c, const float* sens, double* d_acc, cudaStream_t s) {
+  if (n > 0) mlem_update_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, x, c, sens, d_acc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlem_normalise(int64_t n, float* x, float* c, double* d_acc, cudaStream_t s) {
+  if (n > 0) mlem_normalise_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, x, c, d_acc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s) {
+  return cudaMemsetAsync(p, 0, size_t(n) * sizeof(double), s);
+}
+
+}  // namespace raptr

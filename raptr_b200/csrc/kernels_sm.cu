@@ -1,0 +1,658 @@
+// System-matrix rows, ray endpoints and the enclosing-cylinder candidate
+// search, for sm_100a.
+//
+// Row build (one CTA per channel row):
+//   1. thread 0 builds the channel state (both crystal transforms from the
+//      per-angle sine/cosine table, crystal centres, cylinder radius);
+//   2. every thread generates rays r = tid, tid+T, ... (Philox keyed by
+//      (seed, channel)) and walks each through the grid.  The walk visits
+//      exactly the voxels whose intersection length with the ray is positive
+//      and computes that length with the same float operations as the
+//      reference's intersectionLength (src/getSystemMatrixDeviceOnly.cu:129-174):
+//      per-axis plane parameters (face - start)/(end - start), masked max of
+//      the entry parameters, masked min of the exit parameters, and
+//      (exit - entry) * |end - start|.  Lengths are summed into a per-row
+//      open-addressing hash table in shared memory keyed by voxel id;
+//   3. the table is compacted keeping voxels that pass the exact cylinder
+//      test (the reference only evaluates candidates,
+//      src/getSystemMatrixDeviceOnly.cu:433-470), bitonic-sorted by voxel id,
+//      divided by the ray count and written to the row's staging slot.
+// The rows are therefore emitted already in (row, column) order: no global
+// COO sort (src/cooSort.hpp:75-99) and no coo->csr pass are needed; a scan
+// of the row lengths and a gather place them into CSR.
+//
+// This translation unit is compiled with -fmad=false in addition to the
+// explicit round-to-nearest intrinsics used on every exact path.
+#include <climits>
+#include <cstdint>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace raptr {
+
+namespace {
+
+constexpr int kProbeLimit = 128;
+
+__device__ __forceinline__ float plane_alpha(float o, float d, int i, float r0, float dir) {
+  return RFDIV(RFSUB(RFADD(o, RFMUL(float(i), d)), r0), dir);
+}
+
+// Shared-memory accumulation table: keys (voxel id, -1 = empty) and sums.
+template <int H>
+struct RowTable {
+  int* keys;
+  float* vals;
+  int* overflow;
+
+  __device__ __forceinline__ void add(int key, float v) const {
+    constexpr int LOG2H = (H == 2048) ? 11 : (H == 4096) ? 12 : (H == 8192) ? 13 : 14;
+    unsigned h = (unsigned(key) * 2654435761u) >> (32 - LOG2H);
+#pragma unroll 1
+    for (int p = 0; p < kProbeLimit; p++) {
+      int k = reinterpret_cast<volatile int*>(keys)[h];
+      if (k == key) {
+        atomicAdd(&vals[h], v);
+        return;
+      }
+      if (k < 0) {
+        int old = atomicCAS(&keys[h], -1, key);
+        if (old < 0 || old == key) {
+          atomicAdd(&vals[h], v);
+          return;
+        }
+      }
+      h = (h + 1) & (H - 1);
+    }
+    *overflow = 1;
+  }
+};
+
+// Visits every grid voxel whose intersection length with ray r is positive.
+// emit(ix, iy, iz, L) for the common case of a ray that crosses the planes
+// of all three axes; a ray parallel to the planes of some axis (start and
+// end coordinate equal) leaves that axis unconstrained, as the reference's
+// masked min/max does, and every candidate voxel along it gets the length.
+template <class Emit>
+__device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, const float r[6], Emit& emit,
+                                         int* bad_walk) {
+  float dir[3];
+  bool s[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    dir[d] = RFSUB(r[3 + d], r[d]);
+    s[d] = r[d] != r[3 + d];
+  }
+  if (!(s[0] || s[1] || s[2])) return;
+  const float len = norm3_exact(dir[0], dir[1], dir[2]);
+  int step[3] = {0, 0, 0};
+  float amin_g = -INFINITY, amax_g = INFINITY;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    if (s[d]) {
+      step[d] = (r[3 + d] > r[d]) ? 1 : -1;
+      float a0 = plane_alpha(g.o[d], g.d[d], 0, r[d], dir[d]);
+      float a1 = plane_alpha(g.o[d], g.d[d], g.n[d], r[d], dir[d]);
+      amin_g = fmaxf(amin_g, fminf(a0, a1));
+      amax_g = fminf(amax_g, fmaxf(a0, a1));
+    }
+  }
+  if (!(amin_g < amax_g)) return;
+  int id[3];
+  float lo[3], hi[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    id[d] = 0;
+    lo[d] = -INFINITY;
+    hi[d] = INFINITY;
+    if (s[d]) {
+      const int n = g.n[d];
+      float pos = r[d] + amin_g * dir[d];
+      int i = int(floorf((pos - g.o[d]) / g.d[d]));
+      i = min(max(i, 0), n - 1);
+      // Exact correction against the plane parameters: find the voxel whose
+      // interval [lo, hi) contains the entry parameter.
+      float l, h;
+#pragma unroll 1
+      for (int guard = 0; guard < 64; guard++) {
+        float pa = plane_alpha(g.o[d], g.d[d], i, r[d], dir[d]);
+        float pb = plane_alpha(g.o[d], g.d[d], i + 1, r[d], dir[d]);
+        l = step[d] > 0 ? pa : pb;
+        h = step[d] > 0 ? pb : pa;
+        if (!(h > amin_g)) {
+          i += step[d];
+        } else if (l > amin_g) {
+          i -= step[d];
+        } else {
+          break;
+        }
+        if (i < 0 || i >= n) {
+          *bad_walk = 1;
+          return;
+        }
+      }
+      id[d] = i;
+      lo[d] = l;
+      hi[d] = h;
+    }
+  }
+  const bool all3 = s[0] && s[1] && s[2];
+  const int guard_max = g.n[0] + g.n[1] + g.n[2] + 8;
+#pragma unroll 1
+  for (int it = 0; it < guard_max; it++) {
+    float a_lo = fmaxf(lo[0], fmaxf(lo[1], lo[2]));
+    float a_hi = fminf(hi[0], fminf(hi[1], hi[2]));
+    if (a_lo < a_hi) {
+      float L = RFMUL(RFSUB(a_hi, a_lo), len);
+      if (all3) {
+        emit(id[0], id[1], id[2], L);
+      } else {
+        int r0[3], r1[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          r0[d] = s[d] ? id[d] : 0;
+          r1[d] = s[d] ? id[d] : g.n[d] - 1;
+        }
+        for (int a = r0[0]; a <= r1[0]; a++)
+          for (int b = r0[1]; b <= r1[1]; b++)
+            for (int c = r0[2]; c <= r1[2]; c++)
+              if (candidate_test(g, ch, a, b, c)) emit(a, b, c, L);
+      }
+    }
+    if (!(a_hi < amax_g)) return;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      if (s[d] && hi[d] == a_hi) {
+        id[d] += step[d];
+        if (id[d] < 0 || id[d] >= g.n[d]) return;
+        lo[d] = hi[d];
+        hi[d] = plane_alpha(g.o[d], g.d[d], step[d] > 0 ? id[d] + 1 : id[d], r[d], dir[d]);
+      }
+    }
+  }
+  *bad_walk = 1;
+}
+
+// Block-wide exclusive scan of one int per thread; returns the prefix and
+// sets *total.  `warp_sums` holds at least 32 ints.  Ends with a barrier.
+template <int T>
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total, int* warp_sums) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = (lane < T / 32) ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < T / 32) warp_sums[lane] = w;  // inclusive
+  }
+  __syncthreads();
+  int before = (warp > 0 ? warp_sums[warp - 1] : 0) + x - v;
+  *total = warp_sums[T / 32 - 1];
+  __syncthreads();
+  return before;
+}
+
+template <int H, int T>
+__global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __restrict__ sincos,
+                                                    const int32_t* __restrict__ cnl_ids, int64_t row0, int nrays,
+                                                    uint32_t seed, const float* __restrict__ rays,
+                                                    int32_t* __restrict__ st_col, float* __restrict__ st_val,
+                                                    int32_t* __restrict__ row_nnz, int32_t* __restrict__ flags) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int* keys = reinterpret_cast<int*>(smem);
+  float* vals = reinterpret_cast<float*>(smem + H * sizeof(int));
+  __shared__ Channel ch;
+  __shared__ int overflow, bad_walk;
+  __shared__ int warp_sums[32];
+
+  const int tid = threadIdx.x;
+  const int64_t li = row0 + blockIdx.x;
+  const int cnl = cnl_ids[li];
+  if (cnl < 0 || cnl >= num_channels(g)) {
+    if (tid == 0) {
+      row_nnz[blockIdx.x] = -1;
+      atomicOr(flags, 4);
+    }
+    return;
+  }
+
+  for (int i = tid; i < H; i += T) {
+    keys[i] = -1;
+    vals[i] = 0.f;
+  }
+  if (tid == 0) {
+    channel_setup(g, sincos, cnl, ch);
+    overflow = 0;
+    bad_walk = 0;
+  }
+  __syncthreads();
+
+  RowTable<H> table{keys, vals, &overflow};
+  const int nyz = g.n[1] * g.n[2];
+  const int nz = g.n[2];
+  auto emit = [&](int ix, int iy, int iz, float L) { table.add(ix * nyz + iy * nz + iz, L); };
+  for (int ray = tid; ray < nrays; ray += T) {
+    float r[6];
+    if (rays) {
+      const float* src = rays + (li * int64_t(nrays) + ray) * 6;
+#pragma unroll
+      for (int k = 0; k < 6; k++) r[k] = src[k];
+    } else {
+      make_ray(ch, seed, cnl, ray, r);
+    }
+    walk_ray(g, ch, r, emit, &bad_walk);
+  }
+  __syncthreads();
+
+  if (overflow || bad_walk) {
+    if (tid == 0) {
+      row_nnz[blockIdx.x] = -1;
+      atomicOr(flags, overflow ? 1 : 2);
+    }
+    return;
+  }
+
+  // Compaction: keep voxels that pass the cylinder test.
+  constexpr int PER = H / T;
+  int kr[PER];
+  float vr[PER];
+  int cnt = 0;
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    int slot = j * T + tid;
+    int key = keys[slot];
+    float v = vals[slot];
+    bool ok = key >= 0;
+    if (ok) {
+      int ix = key / nyz;
+      int rem = key - ix * nyz;
+      int iy = rem / nz;
+      int iz = rem - iy * nz;
+      ok = candidate_test(g, ch, ix, iy, iz);
+    }
+    kr[j] = ok ? key : -1;
+    vr[j] = v;
+    cnt += ok ? 1 : 0;
+  }
+  int total;
+  int pos = block_exclusive_scan<T>(cnt, &total, warp_sums);
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    if (kr[j] >= 0) {
+      keys[pos] = kr[j];
+      vals[pos] = vr[j];
+      pos++;
+    }
+  }
+  int npad = 1;
+  while (npad < total) npad <<= 1;
+  for (int i = total + tid; i < npad; i += T) keys[i] = INT_MAX;
+  __syncthreads();
+
+  // Bitonic sort of (key, value) by key over [0, npad).
+  for (int k = 2; k <= npad; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = tid; t < (npad >> 1); t += T) {
+        int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+        int p = i | j;
+        bool asc = (i & k) == 0;
+        int ki = keys[i], kp = keys[p];
+        if ((ki > kp) == asc) {
+          keys[i] = kp;
+          keys[p] = ki;
+          float vi = vals[i];
+          vals[i] = vals[p];
+          vals[p] = vi;
+        }
+      }
+      __syncthreads();
+    }
+  }
+
+  const size_t base = size_t(blockIdx.x) * H;
+  const float fr = float(nrays);
+  for (int i = tid; i < total; i += T) {
+    st_col[base + i] = keys[i];
+    st_val[base + i] = RFDIV(vals[i], fr);
+  }
+  if (tid == 0) row_nnz[blockIdx.x] = total;
+}
+
+struct Level {
+  int H, T;
+};
+constexpr Level kLevels[] = {{2048, 128}, {4096, 256}, {8192, 256}, {16384, 512}};
+constexpr int kNumLevels = 4;
+
+template <int H, int T>
+cudaError_t launch_level(const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0, int64_t nrows,
+                         int nrays, uint32_t seed, const float* d_rays, int32_t* st_col, float* st_val,
+                         int32_t* row_nnz, int32_t* d_flags, cudaStream_t s) {
+  const size_t smem = size_t(H) * (sizeof(int) + sizeof(float));
+  cudaError_t e = cudaFuncSetAttribute(sm_rows_kernel<H, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  sm_rows_kernel<H, T><<<unsigned(nrows), T, smem, s>>>(g, d_sincos, d_cnl, row0, nrays, seed, d_rays, st_col,
+                                                         st_val, row_nnz, d_flags);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// CSR placement
+// ---------------------------------------------------------------------------
+
+template <typename TCount>
+__global__ void __launch_bounds__(1024) rows_scan_kernel(const TCount* __restrict__ row_nnz, int64_t n,
+                                                         int64_t* __restrict__ row_ptr, int64_t* __restrict__ d_base) {
+  __shared__ long long warp_sums[32];
+  __shared__ long long carry;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) carry = *d_base;
+  __syncthreads();
+  for (int64_t t0 = 0; t0 < n; t0 += 1024) {
+    int64_t i = t0 + tid;
+    long long v = (i < n) ? (long long)row_nnz[i] : 0;
+    v = v < 0 ? 0 : v;
+    long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      long long w = warp_sums[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        long long y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      warp_sums[lane] = w;
+    }
+    __syncthreads();
+    long long excl = carry + (warp > 0 ? warp_sums[warp - 1] : 0) + x - v;
+    if (i < n) row_ptr[i] = excl;
+    __syncthreads();
+    if (tid == 0) carry += warp_sums[31];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    row_ptr[n] = carry;
+    *d_base = carry;
+  }
+}
+
+__global__ void rows_gather_kernel(const int32_t* __restrict__ st_col, const float* __restrict__ st_val, int slot_cap,
+                                   const int64_t* __restrict__ row_ptr, int64_t nrows, int64_t capacity,
+                                   int32_t* __restrict__ col, float* __restrict__ val) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = w; r < nrows; r += nw) {
+    const int64_t b = row_ptr[r], e = row_ptr[r + 1];
+    const size_t src = size_t(r) * slot_cap;
+    for (int64_t k = lane; k < e - b; k += 32) {
+      if (b + k < capacity) {
+        col[b + k] = st_col[src + k];
+        val[b + k] = st_val[src + k];
+      }
+    }
+  }
+}
+
+// For candidate k of row r (written by the workqueue fill in ascending
+// voxel order), the value from the zero-free staged row, or 0.
+__global__ void expand_kernel(const int32_t* __restrict__ st_col, const float* __restrict__ st_val, int slot_cap,
+                              const int32_t* __restrict__ row_nnz, const int64_t* __restrict__ cand_ptr,
+                              int64_t nrows, const int32_t* __restrict__ cand_vxl, float* __restrict__ out_val) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = w; r < nrows; r += nw) {
+    const int64_t b = cand_ptr[r], e = cand_ptr[r + 1];
+    const int32_t* rc = st_col + size_t(r) * slot_cap;
+    const float* rv = st_val + size_t(r) * slot_cap;
+    const int n = row_nnz[r];
+    for (int64_t k = b + lane; k < e; k += 32) {
+      int v = cand_vxl[k];
+      int lo = 0, hi = n;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (rc[mid] < v) lo = mid + 1;
+        else hi = mid;
+      }
+      out_val[k] = (lo < n && rc[lo] == v) ? rv[lo] : 0.f;
+    }
+  }
+}
+
+__global__ void rays_kernel(DGeom g, const float2* __restrict__ sincos, const int32_t* __restrict__ cnl_ids,
+                            int nrays, uint32_t seed, float* __restrict__ out) {
+  __shared__ Channel ch;
+  const int64_t li = blockIdx.x;
+  const int cnl = cnl_ids[li];
+  if (cnl < 0 || cnl >= num_channels(g)) {
+    for (int64_t k = threadIdx.x; k < int64_t(nrays) * 6; k += blockDim.x) out[li * int64_t(nrays) * 6 + k] = NAN;
+    return;
+  }
+  if (threadIdx.x == 0) channel_setup(g, sincos, cnl, ch);
+  __syncthreads();
+  for (int r = threadIdx.x; r < nrays; r += blockDim.x) {
+    float v[6];
+    make_ray(ch, seed, cnl, r, v);
+    float* dst = out + (li * int64_t(nrays) + r) * 6;
+#pragma unroll
+    for (int k = 0; k < 6; k++) dst[k] = v[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Candidate search: one CTA per list entry, x-slab by x-slab; the voxel
+// rows of a slab that can pass are flattened, tested 256 at a time and the
+// passing voxels compacted in order with warp ballots.
+// ---------------------------------------------------------------------------
+
+constexpr int kWqThreads = 256;
+constexpr int kWqMaxNy = 1024;
+
+template <bool FILL>
+__global__ void __launch_bounds__(kWqThreads) wq_kernel(DGeom g, const float2* __restrict__ sincos,
+                                                        const int32_t* __restrict__ list, int64_t li0,
+                                                        int64_t start_vxl, int64_t* __restrict__ counts,
+                                                        const int64_t* __restrict__ offsets, int64_t max_out,
+                                                        int32_t* __restrict__ out_cnl, int32_t* __restrict__ out_vxl,
+                                                        int32_t* __restrict__ flags) {
+  __shared__ Channel ch;
+  __shared__ int zlo[kWqMaxNy];
+  __shared__ int pre[kWqMaxNy + 1];
+  __shared__ int warp_sums[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int cnl = list[li0 + blockIdx.x];
+  if (cnl < 0 || cnl >= num_channels(g)) {
+    if (tid == 0) {
+      if (!FILL) counts[blockIdx.x] = 0;
+      if (flags) atomicOr(flags, 4);
+    }
+    return;
+  }
+  const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+  const int64_t nyz = int64_t(ny) * nz;
+  int64_t start = (blockIdx.x == 0) ? start_vxl : 0;
+  const int sx = int(start / nyz);
+  const int sy = int((start % nyz) / nz);
+  const int sz = int(start % nz);
+  if (tid == 0) channel_setup(g, sincos, cnl, ch);
+  __syncthreads();
+
+  const int64_t out0 = FILL ? offsets[blockIdx.x] : 0;
+  int64_t count = 0;
+  for (int ix = sx; ix < nx; ix++) {
+    if (FILL && out0 + count >= max_out) break;
+    // Row intervals of this slab; thread t handles rows t, t+T, ...
+    int local = 0;
+    const int per = (ny + kWqThreads - 1) / kWqThreads;
+    int lens[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      lens[q] = 0;
+      int iy = tid * per + q;
+      if (q < per && iy < ny) {
+        int z0 = 0, z1 = -1;
+        bool any = !(ix == sx && iy < sy) && row_z_interval(g, ch, ix, iy, &z0, &z1);
+        if (any && ix == sx && iy == sy) z0 = max(z0, sz);
+        int len = any ? max(z1 - z0 + 1, 0) : 0;
+        zlo[iy] = z0;
+        lens[q] = len;
+        local += len;
+      }
+    }
+    int total;
+    int excl = block_exclusive_scan<kWqThreads>(local, &total, warp_sums);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      int iy = tid * per + q;
+      if (q < per && iy < ny) {
+        pre[iy] = excl;
+        excl += lens[q];
+      }
+    }
+    if (tid == 0) pre[ny] = total;
+    __syncthreads();
+    for (int base = 0; base < total; base += kWqThreads) {
+      int idx = base + tid;
+      bool pass = false;
+      int v = 0;
+      if (idx < total) {
+        int lo = 0, hi = ny;  // last row with pre[row] <= idx
+        while (hi - lo > 1) {
+          int mid = (lo + hi) >> 1;
+          if (pre[mid] <= idx) lo = mid;
+          else hi = mid;
+        }
+        int iy = lo;
+        int iz = zlo[iy] + (idx - pre[iy]);
+        pass = candidate_test(g, ch, ix, iy, iz);
+        v = int(ix * nyz + int64_t(iy) * nz + iz);
+      }
+      unsigned bal = __ballot_sync(0xffffffffu, pass);
+      if (lane == 0) warp_sums[warp] = __popc(bal);
+      __syncthreads();
+      int wpre = 0, btot = 0;
+#pragma unroll
+      for (int w = 0; w < kWqThreads / 32; w++) {
+        int c = warp_sums[w];
+        wpre += (w < warp) ? c : 0;
+        btot += c;
+      }
+      if (FILL && pass) {
+        int64_t p = out0 + count + wpre + __popc(bal & ((1u << lane) - 1u));
+        if (p < max_out) {
+          if (out_cnl) out_cnl[p] = cnl;
+          out_vxl[p] = v;
+        }
+      }
+      count += btot;
+      __syncthreads();
+    }
+  }
+  if (!FILL && tid == 0) counts[blockIdx.x] = count;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+
+int sm_num_levels() { return kNumLevels; }
+int sm_level_capacity(int level) { return kLevels[level].H; }
+int sm_level_threads(int level) { return kLevels[level].T; }
+
+int sm_pick_level(const DGeom& g, int nrays) {
+  long long span = (long long)g.n[0] + g.n[1] + g.n[2];
+  if (nrays <= 128 && span <= 150) return 0;
+  if (span <= 240) return 1;
+  return 2;
+}
+
+cudaError_t launch_sm_rows(int level, const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0,
+                           int64_t nrows, int nrays, uint32_t seed, const float* d_rays, int32_t* st_col,
+                           float* st_val, int32_t* row_nnz, int32_t* d_flags, cudaStream_t s) {
+  if (nrows <= 0) return cudaSuccess;
+  switch (level) {
+    case 0: return launch_level<2048, 128>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, s);
+    case 1: return launch_level<4096, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, s);
+    case 2: return launch_level<8192, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, s);
+    case 3: return launch_level<16384, 512>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_rows_scan(const int32_t* row_nnz, int64_t n, int64_t* row_ptr, int64_t* d_base, cudaStream_t s) {
+  rows_scan_kernel<int32_t><<<1, 1024, 0, s>>>(row_nnz, n, row_ptr, d_base);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows_scan_i64(const int64_t* counts, int64_t n, int64_t* row_ptr, int64_t* d_base, cudaStream_t s) {
+  rows_scan_kernel<int64_t><<<1, 1024, 0, s>>>(counts, n, row_ptr, d_base);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows_gather(const int32_t* st_col, const float* st_val, int slot_cap, const int64_t* row_ptr,
+                               int64_t nrows, int64_t capacity, int32_t* col, float* val, cudaStream_t s) {
+  if (nrows <= 0) return cudaSuccess;
+  int64_t blocks = (nrows * 32 + 255) / 256;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  rows_gather_kernel<<<unsigned(blocks), 256, 0, s>>>(st_col, st_val, slot_cap, row_ptr, nrows, capacity, col, val);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_expand_candidates(const int32_t* st_col, const float* st_val, int slot_cap, const int32_t* row_nnz,
+                                     const int64_t* cand_ptr, int64_t nrows, int32_t* cand_vxl, float* out_val,
+                                     cudaStream_t s) {
+  if (nrows <= 0) return cudaSuccess;
+  int64_t blocks = (nrows * 32 + 255) / 256;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  expand_kernel<<<unsigned(blocks), 256, 0, s>>>(st_col, st_val, slot_cap, row_nnz, cand_ptr, nrows, cand_vxl,
+                                                  out_val);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rays(const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t n, int nrays,
+                        uint32_t seed, float* d_rays, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  rays_kernel<<<unsigned(n), 128, 0, s>>>(g, d_sincos, d_cnl, nrays, seed, d_rays);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wq_count(const DGeom& g, const float2* d_sincos, const int32_t* d_list, int64_t li0, int64_t n,
+                            int64_t start_vxl, int64_t* d_counts, int32_t* d_flags, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (g.n[1] > kWqMaxNy) return cudaErrorInvalidValue;
+  wq_kernel<false><<<unsigned(n), kWqThreads, 0, s>>>(g, d_sincos, d_list, li0, start_vxl, d_counts, nullptr, 0,
+                                                      nullptr, nullptr, d_flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wq_fill(const DGeom& g, const float2* d_sincos, const int32_t* d_list, int64_t li0, int64_t n,
+                           int64_t start_vxl, const int64_t* d_offsets, int64_t max_out, int32_t* d_cnl_out,
+                           int32_t* d_vxl_out, int32_t* d_flags, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (g.n[1] > kWqMaxNy) return cudaErrorInvalidValue;
+  wq_kernel<true><<<unsigned(n), kWqThreads, 0, s>>>(g, d_sincos, d_list, li0, start_vxl, nullptr, d_offsets,
+                                                     max_out, d_cnl_out, d_vxl_out, d_flags);
+  return cudaGetLastError();
+}
+
+}  // namespace raptr

@@ -1,0 +1,156 @@
+// Device-wide scan and sparse-format utilities.
+#include <cstdint>
+
+#include "internal.h"
+
+namespace raptr {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ long long warp_inclusive(long long x) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
+
+// Exclusive block scan of one value per thread (kScanThreads threads).
+__device__ __forceinline__ long long block_excl(long long v, long long* total, long long* ws) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  long long x = warp_inclusive(v);
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    long long w = (lane < kScanThreads / 32) ? ws[lane] : 0;
+    w = warp_inclusive(w);
+    if (lane < kScanThreads / 32) ws[lane] = w;
+  }
+  __syncthreads();
+  long long r = (warp > 0 ? ws[warp - 1] : 0) + x - v;
+  *total = ws[kScanThreads / 32 - 1];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_partials(const int64_t* __restrict__ in, int64_t n,
+                                                              int64_t* __restrict__ partial) {
+  __shared__ long long ws[32];
+  const int64_t base = int64_t(blockIdx.x) * kScanTile + int64_t(threadIdx.x) * kScanItems;
+  long long s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++)
+    if (base + k < n) s += in[base + k];
+  long long tot;
+  block_excl(s, &tot, ws);
+  if (threadIdx.x == 0) partial[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_spine(int64_t* __restrict__ partial, int64_t nb) {
+  __shared__ long long ws[32];
+  __shared__ long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int64_t t0 = 0; t0 < nb; t0 += kScanThreads) {
+    int64_t i = t0 + threadIdx.x;
+    long long v = (i < nb) ? partial[i] : 0;
+    long long tot;
+    long long ex = block_excl(v, &tot, ws);
+    if (i < nb) partial[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[nb] = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_apply(const int64_t* __restrict__ in, int64_t n,
+                                                           const int64_t* __restrict__ partial,
+                                                           int64_t* __restrict__ out, int64_t nb) {
+  __shared__ long long ws[32];
+  const int64_t base = int64_t(blockIdx.x) * kScanTile + int64_t(threadIdx.x) * kScanItems;
+  long long v[kScanItems];
+  long long s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    s += v[k];
+  }
+  long long tot;
+  long long ex = block_excl(s, &tot, ws) + partial[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    if (base + k < n) out[base + k] = ex;
+    ex += v[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = partial[nb];
+}
+
+__global__ void coo2csr_kernel(const int32_t* __restrict__ rows, int64_t nnz, int64_t m, int64_t* __restrict__ rp) {
+  for (int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; r <= m; r += int64_t(gridDim.x) * blockDim.x) {
+    int64_t lo = 0, hi = nnz;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (rows[mid] < r) lo = mid + 1;
+      else hi = mid;
+    }
+    rp[r] = lo;
+  }
+}
+
+__global__ void csr2ecsr_kernel(int64_t* __restrict__ ecsr, const int32_t* __restrict__ yrow, int64_t nnzr,
+                                const int64_t* __restrict__ csr, int64_t m) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i <= nnzr; i += int64_t(gridDim.x) * blockDim.x)
+    ecsr[i] = (i < nnzr) ? csr[yrow[i]] : csr[m];
+}
+
+__global__ void iota_kernel(int32_t* __restrict__ p, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    p[i] = int32_t(i);
+}
+
+unsigned grid_for(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > 148 * 32) b = 148 * 32;
+  return unsigned(b);
+}
+
+}  // namespace
+
+cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s) {
+  if (n > 0) iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, n);
+  return cudaGetLastError();
+}
+
+int64_t scan_temp_elems(int64_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
+
+cudaError_t launch_scan_i64(const int64_t* in, int64_t n, int64_t* out, int64_t* temp, cudaStream_t s) {
+  int64_t nb = (n + kScanTile - 1) / kScanTile;
+  if (nb == 0) {
+    return cudaMemsetAsync(out, 0, sizeof(int64_t), s);
+  }
+  scan_partials<<<unsigned(nb), kScanThreads, 0, s>>>(in, n, temp);
+  scan_spine<<<1, kScanThreads, 0, s>>>(temp, nb);
+  scan_apply<<<unsigned(nb), kScanThreads, 0, s>>>(in, n, temp, out, nb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_coo2csr(const int32_t* rows, int64_t nnz, int64_t m, int64_t* row_ptr, int64_t*, cudaStream_t s) {
+  coo2csr_kernel<<<grid_for(m + 1, 256), 256, 0, s>>>(rows, nnz, m, row_ptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_csr2ecsr(int64_t* ecsr, const int32_t* yrow, int64_t nnzr, const int64_t* csr, int64_t m,
+                            cudaStream_t s) {
+  csr2ecsr_kernel<<<grid_for(nnzr + 1, 256), 256, 0, s>>>(ecsr, yrow, nnzr, csr, m);
+  return cudaGetLastError();
+}
+
+}  // namespace raptr

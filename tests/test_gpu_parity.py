@@ -1,0 +1,380 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bars: bit-exact for integer/index work (candidates, CSR structure, ray
+endpoints); matrix values within 1e-5 relative of the oracle given identical
+rays (the GPU sums rays in a different order); MLEM images within 1e-4
+relative L2 of the FP32 oracle.
+"""
+import numpy as np
+import pytest
+
+from raptr_b200 import config as cfg
+
+pytestmark = pytest.mark.gpu
+
+SEED = 1251
+VAL_RTOL = 1e-5
+IMG_RTOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+@pytest.fixture(scope="module")
+def ctx_small(rlib, torch):
+    return rlib.Context(cfg.SMALL, 0)
+
+
+@pytest.fixture(scope="module")
+def ctx_full(rlib, torch):
+    return rlib.Context(cfg.FULL, 0)
+
+
+def assert_rows_equal(rp_g, col_g, val_g, rp_o, col_o, val_o, rtol=VAL_RTOL):
+    assert np.array_equal(rp_g, rp_o), "row pointers differ"
+    assert np.array_equal(col_g, col_o), "columns differ"
+    if val_o.size:
+        err = np.abs(val_g.astype(np.float64) - val_o) / np.maximum(np.abs(val_o.astype(np.float64)), 1e-30)
+        assert err.max() <= rtol, f"max rel err {err.max()}"
+
+
+# ---------------------------------------------------------------- rays
+
+@pytest.mark.parametrize("which", ["small", "full", "fine"])
+def test_rays_bit_exact(rlib, oracle, torch, which):
+    g = {"small": cfg.SMALL, "full": cfg.FULL, "fine": cfg.FINE}[which]
+    ctx = rlib.Context(g, 0)
+    rng = np.random.Generator(np.random.PCG64(11))
+    lst = np.unique(np.concatenate([rng.integers(0, g.n_channels, 200), [0, g.n_channels - 1]])).astype(np.int32)
+    got = ctx.rays(lst, 64, SEED).cpu().numpy()
+    want = oracle.rays(g, lst, 64, SEED)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+# ---------------------------------------------------------------- candidates
+
+def test_workqueue_matches_reference_golden(rlib, golden, ctx_small):
+    c, v, cur = ctx_small.workqueue(golden["small_list"], max_out=1 << 20)
+    assert np.array_equal(c.cpu().numpy(), golden["small_cnl"])
+    assert np.array_equal(v.cpu().numpy(), golden["small_vxl"])
+    assert cur == (golden["small_list"].size, 0)
+
+
+def test_workqueue_cursor_chunks_match_reference(rlib, golden, ctx_small):
+    cur = (0, 0)
+    k = 0
+    for n, cnt, want_cur in zip(golden["wq_sizes"], golden["wq_counts"], golden["wq_cursors"]):
+        c, v, cur = ctx_small.workqueue(golden["wq_list"], cursor=cur, max_out=int(n))
+        assert c.numel() == cnt
+        assert np.array_equal(c.cpu().numpy(), golden["wq_cnl"][k:k + cnt])
+        assert np.array_equal(v.cpu().numpy(), golden["wq_vxl"][k:k + cnt])
+        assert tuple(cur) == tuple(want_cur)
+        k += cnt
+
+
+def test_workqueue_many_channels_bit_exact(rlib, oracle, ctx_small):
+    g = cfg.SMALL
+    lst = np.arange(0, g.n_channels, 41, dtype=np.int32)
+    c, v, cur = ctx_small.workqueue(lst, max_out=lst.size * 6000)
+    co, vo, curo = oracle.workqueue(g, lst)
+    assert np.array_equal(c.cpu().numpy(), co) and np.array_equal(v.cpu().numpy(), vo)
+    assert cur == curo
+
+
+def test_workqueue_full_geometry_bit_exact(rlib, oracle, ctx_full):
+    g = cfg.FULL
+    rng = np.random.Generator(np.random.PCG64(5))
+    lst = rng.integers(0, g.n_channels, 120).astype(np.int32)
+    c, v, cur = ctx_full.workqueue(lst, max_out=lst.size * 20000)
+    co, vo, curo = oracle.workqueue(g, lst)
+    assert np.array_equal(c.cpu().numpy(), co) and np.array_equal(v.cpu().numpy(), vo)
+    counts = ctx_full.candidate_counts(lst).cpu().numpy()
+    assert np.array_equal(counts, oracle.candidate_counts(g, lst))
+
+
+def test_workqueue_edge_cases(rlib, oracle, ctx_small):
+    g = cfg.SMALL
+    lst = np.array([7, 8], np.int32)
+    # max_out = 0 leaves the cursor untouched
+    c, v, cur = ctx_small.workqueue(lst, cursor=(1, 5), max_out=0)
+    assert c.numel() == 0 and cur == (1, 5)
+    # empty list
+    c, v, cur = ctx_small.workqueue(np.zeros(0, np.int32), max_out=10)
+    assert c.numel() == 0 and cur == (0, 0)
+    # cursor in the middle of a row, and at the last voxel
+    for start in [(0, 31000), (1, g.n_voxels - 1), (2, 0)]:
+        c, v, cur = ctx_small.workqueue(lst, cursor=start, max_out=100000)
+        co, vo, curo = oracle.workqueue(g, lst, cursor=start)
+        assert np.array_equal(c.cpu().numpy(), co) and np.array_equal(v.cpu().numpy(), vo) and cur == curo
+    # a limit that ends exactly at the last candidate of the first channel
+    co, vo, _ = oracle.workqueue(g, lst[:1])
+    c, v, cur = ctx_small.workqueue(lst, max_out=co.size)
+    _, _, curo = oracle.workqueue(g, lst, max_out=co.size)
+    assert cur == curo
+
+
+# ---------------------------------------------------------------- system matrix
+
+@pytest.fixture(scope="module")
+def small_full_matrix(rlib, oracle, ctx_small):
+    g = cfg.SMALL
+    lst = np.arange(g.n_channels, dtype=np.int32)
+    A = ctx_small.build(lst, 100, SEED)
+    rp, col, val = oracle.sysmat(g, lst, 100, SEED, method=1)
+    return A, (rp, col, val), lst
+
+
+def test_sysmat_small_all_channels(small_full_matrix):
+    A, (rp, col, val), lst = small_full_matrix
+    assert A.m == lst.size and A.nnz == col.size
+    assert_rows_equal(*A.to_numpy(), rp, col, val)
+
+
+def test_sysmat_keep_zeros_matches_reference_golden(rlib, golden, ctx_small):
+    A = ctx_small.build(golden["small_list"], 100, SEED, keep_zeros=True)
+    rp, col, val = A.to_numpy()
+    assert np.array_equal(np.repeat(golden["small_list"], np.diff(rp)), golden["small_cnl"])
+    assert np.array_equal(col, golden["small_vxl"])
+    want = golden["small_val"].astype(np.float64)
+    assert np.all((val == 0) == (want == 0))
+    nz = want != 0
+    assert np.max(np.abs(val[nz] - want[nz]) / want[nz]) <= VAL_RTOL
+
+
+def test_sysmat_full_geometry_golden_rows(rlib, golden, ctx_full):
+    A = ctx_full.build(golden["full_list"], 64, SEED, keep_zeros=True)
+    rp, col, val = A.to_numpy()
+    assert np.array_equal(col, golden["full_vxl"])
+    want = golden["full_val"].astype(np.float64)
+    assert np.all((val == 0) == (want == 0))
+    nz = want != 0
+    assert np.max(np.abs(val[nz] - want[nz]) / want[nz]) <= VAL_RTOL
+
+
+def test_sysmat_full_geometry_1000_rays(rlib, oracle, ctx_full):
+    g = cfg.FULL
+    rng = np.random.Generator(np.random.PCG64(8))
+    lst = rng.integers(0, g.n_channels, 300).astype(np.int32)
+    A = ctx_full.build(lst, 1000, SEED)
+    assert_rows_equal(*A.to_numpy(), *oracle.sysmat(g, lst, 1000, SEED, method=1))
+
+
+def test_sysmat_fine_geometry(rlib, oracle):
+    g = cfg.FINE
+    ctx = rlib.Context(g, 0)
+    rng = np.random.Generator(np.random.PCG64(9))
+    lst = rng.integers(0, g.n_channels, 60).astype(np.int32)
+    A = ctx.build(lst, 1000, SEED)
+    assert_rows_equal(*A.to_numpy(), *oracle.sysmat(g, lst, 1000, SEED, method=1))
+
+
+def test_sysmat_given_rays_with_axis_parallel_rays(rlib, oracle, torch, ctx_small):
+    # Identical caller-supplied endpoints, including rays parallel to a plane
+    # family, against the reference algorithm (method 0).
+    g = cfg.SMALL
+    lst = np.array([40000, 40001, 71234], np.int32)
+    rays = oracle.rays(g, lst, 32, 5)
+    rays[0, :, 4] = rays[0, :, 1]
+    rays[1, :10, 5] = rays[1, :10, 2]
+    A = ctx_small.build(lst, 32, 0, rays=torch.from_numpy(rays))
+    assert_rows_equal(*A.to_numpy(), *oracle.sysmat(g, lst, 32, 0, rays_in=rays, method=0))
+
+
+def test_sysmat_duplicate_and_unordered_list(rlib, oracle, ctx_small):
+    g = cfg.SMALL
+    lst = np.array([99, 5, 99, 142804, 0], np.int32)
+    A = ctx_small.build(lst, 100, SEED)
+    assert_rows_equal(*A.to_numpy(), *oracle.sysmat(g, lst, 100, SEED, method=1))
+
+
+def test_sysmat_caller_buffers_two_phase(rlib, oracle, torch, ctx_small):
+    g = cfg.SMALL
+    lst = np.arange(1000, 1400, dtype=np.int32)
+    rp_o, col_o, val_o = oracle.sysmat(g, lst, 100, SEED, method=1)
+    rp = torch.empty(lst.size + 1, dtype=torch.int64, device="cuda")
+    col = torch.empty(10, dtype=torch.int32, device="cuda")
+    val = torch.empty(10, dtype=torch.float32, device="cuda")
+    st, nnz = ctx_small.build_into(lst, 100, SEED, rp, col, val)
+    assert st == rlib.RAPTR_ERR_CAPACITY and nnz == col_o.size
+    assert np.array_equal(rp.cpu().numpy(), rp_o)
+    col = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    val = torch.empty(nnz, dtype=torch.float32, device="cuda")
+    st, nnz2 = ctx_small.build_into(lst, 100, SEED, rp, col, val)
+    assert st == 0 and nnz2 == nnz
+    assert_rows_equal(rp.cpu().numpy(), col.cpu().numpy(), val.cpu().numpy(), rp_o, col_o, val_o)
+
+
+def test_sysmat_empty_list(rlib, ctx_small):
+    A = ctx_small.build(np.zeros(0, np.int32), 100, SEED)
+    assert A.m == 0 and A.nnz == 0 and A.row_ptr.cpu().tolist() == [0]
+
+
+def test_invalid_arguments_raise(rlib, ctx_small):
+    with pytest.raises(rlib.RaptrError):
+        ctx_small.build(np.array([1], np.int32), 0, SEED)
+
+
+# ---------------------------------------------------------------- SpMV / ops
+
+def test_spmv_forward_and_back(rlib, oracle, torch, small_full_matrix):
+    A, (rp, col, val), lst = small_full_matrix
+    g = cfg.SMALL
+    rng = np.random.Generator(np.random.PCG64(2))
+    x = rng.random(g.n_voxels).astype(np.float32)
+    e = rng.random(A.m).astype(np.float32)
+    yt = rlib.spmv(rlib.OP_N, A.m, A.n, A.row_ptr, A.col, A.val, torch.from_numpy(x).cuda()).cpu().numpy()
+    want = oracle.spmv(0, A.m, A.n, rp, col, val, x.astype(np.float64), dtype=np.float64)
+    assert np.max(np.abs(yt - want) / np.maximum(np.abs(want), 1e-30)) < 1e-5
+    c0 = rng.random(g.n_voxels).astype(np.float32)
+    c = rlib.spmv(rlib.OP_T, A.m, A.n, A.row_ptr, A.col, A.val, torch.from_numpy(e).cuda(), alpha=2.0, beta=0.5,
+                  y=torch.from_numpy(c0.copy()).cuda()).cpu().numpy()
+    want = oracle.spmv(1, A.m, A.n, rp, col, val, e.astype(np.float64), alpha=2.0, beta=0.5,
+                       y=c0.astype(np.float64), dtype=np.float64)
+    assert np.max(np.abs(c - want) / np.maximum(np.abs(want), 1e-30)) < 1e-5
+
+
+def test_mlem_operations_known_answers(rlib, golden, torch):
+    n = 10
+    A = torch.tensor(((np.arange(n) + 1) ** 2).astype(np.float32)).cuda()
+    B = torch.full((n,), 10.0, device="cuda")
+    Cc = torch.arange(1, n + 1, dtype=torch.float32, device="cuda")
+    D = torch.zeros(n, device="cuda")
+    rlib.divides(D, A, Cc)
+    assert np.array_equal(D.cpu().numpy(), golden["mlem_divides"])
+    rlib.divides_multiplies(D, A, B, Cc)
+    assert np.array_equal(D.cpu().numpy(), golden["mlem_divmul"])
+    assert rlib.vsum(D) == 550.0
+    rlib.scales(D, float(np.float32(1.0 / 550.0)))
+    assert np.array_equal(D.cpu().numpy(), golden["mlem_scaled"])
+    z = torch.tensor([0.0, 2.0], device="cuda")
+    rlib.divides_multiplies(D[:2], torch.tensor([2.0, 3.0], device="cuda"), torch.tensor([5.0, 7.0], device="cuda"), z)
+    assert D[:2].cpu().tolist() == [10.0, 10.5]
+
+
+def test_coo2csr_and_ecsr_known_answers(rlib, torch):
+    rows = torch.tensor([0, 1, 1, 1, 2, 2, 3, 3, 3], dtype=torch.int32, device="cuda")
+    assert rlib.coo2csr(rows, 4).cpu().tolist() == [0, 1, 4, 6, 9]
+    e = rlib.csr2ecsr(torch.tensor([2, 4, 6], dtype=torch.int32, device="cuda"),
+                      torch.tensor([0, 0, 0, 3, 3, 3, 3, 5], dtype=torch.int64, device="cuda"))
+    assert e.cpu().tolist() == [0, 3, 3, 5]
+
+
+def test_sensitivity_fp64(rlib, oracle, small_full_matrix):
+    A, (rp, col, val), lst = small_full_matrix
+    s64, s32 = rlib.sensitivity(A)
+    want = oracle.column_sums_f64(A.m, A.n, rp, col, val)
+    s64 = s64.cpu().numpy()
+    assert np.max(np.abs(s64 - want)) <= 1e-9 * want.max()
+    np.testing.assert_allclose(s32.cpu().numpy(), (want / want.sum()).astype(np.float32), rtol=1e-6, atol=1e-12)
+
+
+# ---------------------------------------------------------------- MLEM
+
+@pytest.fixture(scope="module")
+def small_measurement(small_full_matrix):
+    A, (rp, col, val), lst = small_full_matrix
+    g = cfg.SMALL
+    xt = cfg.phantom(g, rods=False)
+    from oracle import oracle as O
+
+    lam = O.spmv(0, A.m, A.n, rp, col, val, xt.astype(np.float64), dtype=np.float64)
+    y = cfg.poisson_measurement(lam, 2e6, seed=7)
+    return y
+
+
+def test_mlem_matches_oracle(rlib, oracle, torch, ctx_small, small_full_matrix, small_measurement):
+    A, (rp, col, val), lst = small_full_matrix
+    y = small_measurement
+    meas = y != 0
+    # the oracle uses only measured rows (the reference's matrix has no others)
+    rows = np.nonzero(meas)[0]
+    rp_m = np.concatenate([[0], np.cumsum(np.diff(rp)[rows])]).astype(np.int64)
+    col_m = np.concatenate([col[rp[r]:rp[r + 1]] for r in rows]).astype(np.int32)
+    val_m = np.concatenate([val[rp[r]:rp[r + 1]] for r in rows]).astype(np.float32)
+    s_all = oracle.column_sums_f64(A.m, A.n, rp, col, val)
+    s = (s_all / s_all.sum()).astype(np.float32)
+    n = A.n
+    x0 = np.full(n, np.float32(1.0 / n), np.float32)
+    want32 = oracle.mlem(rows.size, n, rp_m, col_m, val_m, y[rows], s, x0, 20)
+    want64 = oracle.mlem(rows.size, n, rp_m, col_m, val_m, y[rows].astype(np.float64), s.astype(np.float64),
+                         x0.astype(np.float64), 20, dtype=np.float64)
+    for use_graph in (False, True):
+        x = torch.from_numpy(x0.copy()).cuda()
+        ll = ctx_small.mlem(A, torch.from_numpy(y).cuda(), torch.from_numpy(s).cuda(), x, 20, use_graph=use_graph,
+                            loglik=True)
+        x = x.cpu().numpy()
+        assert np.linalg.norm(x - want32) / np.linalg.norm(want32) < IMG_RTOL
+        assert np.linalg.norm(x - want64) / np.linalg.norm(want64) < IMG_RTOL
+        assert abs(float(x.sum()) - 1.0) < 1e-5
+        assert np.all(np.diff(ll) >= -1e-6 * abs(ll[-1]))  # MLEM never decreases the likelihood
+
+
+def test_mlem_half_steps_equal_full_iteration(rlib, torch, ctx_small, small_full_matrix, small_measurement):
+    A, _, _ = small_full_matrix
+    y = torch.from_numpy(small_measurement).cuda()
+    s64, s = rlib.sensitivity(A)
+    n = A.n
+    x1 = torch.full((n,), 1.0 / n, device="cuda")
+    x2 = x1.clone()
+    ctx_small.mlem(A, y, s, x1, 3, use_graph=False)
+    c = torch.zeros(n, device="cuda")
+    acc = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        rlib.mlem_project(A, y, x2, c)
+        rlib.mlem_update(x2, c, s, acc)
+    assert torch.linalg.norm(x1 - x2) / torch.linalg.norm(x1) < 1e-6
+
+
+def test_reco_host_end_to_end(rlib, oracle, torch, small_full_matrix, small_measurement):
+    A, _, _ = small_full_matrix
+    g = cfg.SMALL
+    y = small_measurement
+    x, st = rlib.reco_host(g, y, 100, SEED, 20)
+    s64, s = rlib.sensitivity(A)
+    xr = torch.full((A.n,), np.float32(1.0 / A.n), device="cuda")
+    rlib.Context(g, 0).mlem(A, torch.from_numpy(y).cuda(), s, xr, 20)
+    xr = xr.cpu().numpy()
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < IMG_RTOL
+    assert st["nnz"] == A.nnz and st["h2d_bytes"] >= y.nbytes and st["d2h_bytes"] == x.nbytes
+    assert st["build_ms"] > 0 and st["iter_ms"] > 0
+
+
+# ---------------------------------------------------------------- full-size properties
+
+def test_full_size_matrix_properties(rlib, oracle, torch, ctx_full):
+    """The whole 70^3 x 5.14M-channel matrix: structural invariants and a
+    checksum of a row sample against the oracle (size-independent checks)."""
+    g = cfg.FULL
+    lst = np.arange(g.n_channels, dtype=np.int32)
+    A = ctx_full.build(lst, 1000, SEED)
+    rp = A.row_ptr
+    assert int(rp[0]) == 0 and int(rp[-1]) == A.nnz
+    assert bool((rp[1:] >= rp[:-1]).all())
+    assert int(A.col.min()) >= 0 and int(A.col.max()) < g.n_voxels
+    assert bool((A.val > 0).all())
+    rng = np.random.Generator(np.random.PCG64(77))
+    sample = np.sort(rng.choice(g.n_channels, 64, replace=False)).astype(np.int32)
+    rp_o, col_o, val_o = oracle.sysmat(g, sample, 1000, SEED, method=1)
+    rp_h = rp.cpu().numpy()
+    for k, r in enumerate(sample):
+        b, e = rp_h[r], rp_h[r + 1]
+        cg = A.col[b:e].cpu().numpy()
+        vg = A.val[b:e].cpu().numpy()
+        assert np.array_equal(cg, col_o[rp_o[k]:rp_o[k + 1]])
+        assert np.max(np.abs(vg - val_o[rp_o[k]:rp_o[k + 1]]) / val_o[rp_o[k]:rp_o[k + 1]]) <= VAL_RTOL
+        assert np.all(np.diff(cg) > 0)
+    # a checksum of checksums: row sums (A * ones), column sums (FP64
+    # sensitivity) and the plain sum of all values agree
+    total = 0.0
+    chunk = 1 << 28
+    for i in range(0, A.nnz, chunk):
+        total += float(A.val[i:i + chunk].double().sum())
+    row_sums = rlib.spmv(rlib.OP_N, A.m, A.n, A.row_ptr, A.col, A.val, torch.ones(A.n, device="cuda"))
+    assert abs(float(row_sums.double().sum()) - total) <= 1e-5 * total
+    s64, s = rlib.sensitivity(A)
+    assert abs(float(s64.sum()) - total) <= 1e-9 * total
