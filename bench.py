@@ -1,0 +1,477 @@
+#!/usr/bin/env python
+"""Benchmark of the raptr reconstruction hot path on B200.
+
+Workload (default): the full ePET configuration -- 70^3 voxels of 2 mm,
+180 angles x 13^4 crystal pairs = 5,140,980 channels, 1000 Monte Carlo rays
+per channel, a two-sphere + five-rod phantom with 1e8 Poisson counts, 50
+MLEM iterations from a uniform image.  Data are synthetic (seeded).
+
+One step = one whole reconstruction job from the measurement resident in
+HBM: system-matrix build for all channels (CSR), its transpose (CSC), the
+FP64 sensitivity image, and 50 MLEM iterations.  The reported metric is MLEM
+iterations per second of that job (50 / job time), so the matrix build is
+inside the timed region (the reference rebuilds the matrix in every
+iteration, src/tests/reco.cu:230-252); matrix_build_s and the resident
+per-iteration rate are reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl raptr|reference]
+
+With N > 1 (torchrun, one rank per GPU) the channel rows are sharded over
+the ranks (strong scaling of the same job); each iteration all-reduces the
+N-voxel back projection over NCCL, as the reference does over MPI
+(src/tests/reco.cu:237-281).
+
+--impl reference times the reference's own CPU algorithm (candidate search,
+per-candidate mean intersection length over all rays, CSR SpMVs; built from
+the reference sources into oracle/_ref) on a bounded channel sample on all
+host cores, extrapolated by channel count to the same job.
+"""
+from __future__ import annotations
+
+import argparse
+import gc
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from raptr_b200 import config as cfg  # noqa: E402
+
+SEED = 1251
+MEAS_SEED = 20240
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["raptr", "reference"], default="raptr")
+    p.add_argument("--workload", choices=list(cfg.WORKLOADS), default="full")
+    p.add_argument("--cpu-sample-s", type=float, default=12.0, help="CPU seconds for the cpu_baseline sample")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(name):
+    w = dict(cfg.WORKLOADS[name])
+    w["name"] = name
+    return w
+
+
+def config_of(w, n_gpus):
+    g = w["geom"]
+    return {
+        "workload": f"ePET {g.grid_n[0]}^3 x {g.grid_d[0] * 1e3:g} mm, {g.na} angles x 13^4 crystal pairs = "
+                    f"{g.n_channels} channels, {w['nrays']} rays/channel, {w['counts']:.0e} counts, "
+                    f"{w['niter']} MLEM iterations",
+        "voxels": g.n_voxels,
+        "channels": g.n_channels,
+        "rays_per_channel": w["nrays"],
+        "counts": w["counts"],
+        "iterations": w["niter"],
+        "parallelism": f"row-shard x{n_gpus}" if n_gpus > 1 else "single GPU",
+        "l2": "inputs larger than L2 (system matrix ~30 GB CSR + ~30 GB CSC)",
+        "phantom": "background 0.1, sphere r15 mm 1.0, sphere r8 mm at +20 mm x 4.0" +
+                   (", 5 rods r2-6 mm 2.0" if w["rods"] else ""),
+    }
+
+
+def metric_name(w):
+    g = w["geom"]
+    return (f"MLEM iterations/s, whole job incl. system-matrix build ({g.grid_n[0]}^3 voxels, "
+            f"{g.n_channels / 1e6:.2f}M channels, {w['nrays']} rays)")
+
+
+# ---------------------------------------------------------------------------
+# Clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200", "-i",
+                 self.gpu_id], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s, p in zip(sm, power) if p > 0.25 * max(power)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power)}
+
+
+def gpu_id_for(torch, dev):
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:  # noqa: BLE001
+        return str(dev)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "of measured"
+    return 6650.0, "of fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (reference harness or oracle port)
+# ---------------------------------------------------------------------------
+
+def cpu_reference_sample(w, budget_s: float, threads: int):
+    """Times the reference algorithm on a channel sample (all host threads):
+    candidates by getWorkqueue, each element the mean over all rays of
+    intersectionLength, then the two CSR SpMVs of an iteration over the
+    sample's rows (the reference's COO keeps every candidate).  Returns
+    (per-channel build seconds, per-entry SpMV seconds, entries per channel,
+    kind, channels sampled, threads)."""
+    import ctypes as C
+
+    from oracle import oracle as O
+
+    g = w["geom"]
+    nrays = w["nrays"]
+    kind = "reference" if O.ref_available() else "port"
+    rng = np.random.Generator(np.random.PCG64(99))
+    sample = rng.permutation(g.n_channels).astype(np.int32)
+    og = O.to_ogeom(g)
+    per_call = 2
+
+    def run_ref(chs):
+        U = O.ray_uniforms_batch(SEED, chs, nrays)
+        cap = int(len(chs) * 40000)
+        oc = np.zeros(cap, np.int32)
+        ov = np.zeros(cap, np.int32)
+        oval = np.zeros(cap, np.float32)
+        n = O.ref().ref_sysmat(C.byref(og), chs, len(chs), nrays, U, cap, oc, ov, oval)
+        return int(n), oc[:n], ov[:n], oval[:n]
+
+    def run_port(chs):
+        rp, col, val = O.sysmat(g, chs, nrays, SEED, method=0, keep_zeros=True, nthreads=1)
+        return int(col.size), np.repeat(chs, np.diff(rp)), col, val
+
+    fn = run_ref if kind == "reference" else run_port
+    done, entries, t0 = 0, 0, time.perf_counter()
+    rows_c, rows_v, rows_val = [], [], []
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        while time.perf_counter() - t0 < budget_s:
+            chunk = [sample[done + i * per_call: done + (i + 1) * per_call] for i in range(threads)]
+            for n, oc, ov, oval in ex.map(fn, chunk):
+                entries += n
+                if len(rows_c) < 64:
+                    rows_c.append(oc)
+                    rows_v.append(ov)
+                    rows_val.append(oval)
+            done += threads * per_call
+    t_build = time.perf_counter() - t0
+    # SpMV cost per entry on the sampled rows (single thread, scaled by threads)
+    cnl = np.concatenate(rows_c)
+    col = np.concatenate(rows_v).astype(np.int32)
+    val = np.concatenate(rows_val).astype(np.float32)
+    _, inv = np.unique(cnl, return_inverse=True)
+    order = np.lexsort((col, inv))
+    rows = inv[order].astype(np.int32)
+    rp = O.coo2csr(rows, int(rows.max()) + 1)
+    x = np.ones(g.n_voxels, np.float32)
+    t1 = time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t1 < 0.5:
+        ycol = O.spmv(0, rp.size - 1, g.n_voxels, rp, col[order], val[order], x)
+        O.spmv(1, rp.size - 1, g.n_voxels, rp, col[order], val[order], ycol)
+        reps += 1
+    t_spmv_entry = (time.perf_counter() - t1) / reps / max(col.size, 1) / 2 / threads
+    return t_build * threads / done, t_spmv_entry, entries / done, kind, done, threads
+
+
+def cpu_job_rate(w, budget_s, threads):
+    """MLEM iterations/s of the reference's job on the host cores: every
+    iteration rebuilds the matrix of all measured channels and runs two
+    SpMVs over it (src/tests/reco.cu:230-281)."""
+    g = w["geom"]
+    per_ch, per_entry, ent_per_ch, kind, nsamp, thr = cpu_reference_sample(w, budget_s, threads)
+    t_build = per_ch * g.n_channels / thr
+    t_spmv = 2 * per_entry * ent_per_ch * g.n_channels
+    t_iter = t_build + t_spmv
+    return {
+        "value": 1.0 / t_iter,
+        "unit": "MLEM iterations/s",
+        "cores": thr,
+        "kind": kind,
+        "sample": f"{nsamp} random channels x {w['nrays']} rays on {thr} threads ({budget_s:.0f} s), "
+                  f"extrapolated by channel count to {g.n_channels} channels; one iteration = rebuild "
+                  f"({t_build:.3g} s) + 2 SpMVs over {ent_per_ch:.0f} entries/channel ({t_spmv:.3g} s)",
+        "matrix_build_s": t_build,
+    }
+
+
+# ---------------------------------------------------------------------------
+# The GPU job
+# ---------------------------------------------------------------------------
+
+def synth_measurement(R, torch, ctx, w, lst, dist=None):
+    """Seeded Poisson measurement of the phantom through the system matrix
+    (setup, not timed).  Each rank projects its own rows; the expected counts
+    are gathered so that every rank draws the same measurement."""
+    g = w["geom"]
+    A = ctx.build(lst, w["nrays"], SEED)
+    xt = torch.from_numpy(cfg.phantom(g, w["rods"])).cuda()
+    lam = R.spmv(R.OP_N, A.m, A.n, A.row_ptr, A.col, A.val, xt)
+    del A
+    gc.collect()
+    if dist is not None:
+        world = dist.get_world_size()
+        sizes = [(r + 1) * g.n_channels // world - r * g.n_channels // world for r in range(world)]
+        parts = [torch.empty(n, device="cuda") for n in sizes]
+        dist.all_gather(parts, lam)
+        lam = torch.cat(parts)
+    torch.cuda.synchronize()
+    return cfg.poisson_measurement(lam.cpu().numpy(), w["counts"], MEAS_SEED)
+
+
+def run_job(R, torch, ctx, w, lst, y_dev, dist=None):
+    """One reconstruction job; returns per-phase device times (ms) and the
+    per-iteration kernel times."""
+    g = w["geom"]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    ev[0].record()
+    A = ctx.build(lst, w["nrays"], SEED)
+    ev[1].record()
+    A.transpose()
+    ev[2].record()
+    s64, s = R.sensitivity(A)
+    if dist is not None:
+        dist.all_reduce(s64)
+        s = (s64 / s64.sum()).float()
+    ev[3].record()
+    x = torch.full((g.n_voxels,), np.float32(1.0 / g.n_voxels), device="cuda")
+    if dist is None:
+        kt = ctx.mlem(A, y_dev, s, x, w["niter"], use_graph=False, kernel_times=True)
+    else:
+        e = torch.empty(A.m, device="cuda")
+        c = torch.empty(g.n_voxels, device="cuda")
+        acc = torch.zeros(1, dtype=torch.float64, device="cuda")
+        kev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(w["niter"])]
+        for it in range(w["niter"]):
+            kev[it][0].record()
+            R.mlem_forward(A, y_dev, x, e)
+            kev[it][1].record()
+            R.mlem_back(A, e, c)
+            kev[it][2].record()
+            dist.all_reduce(c)
+            R.mlem_update(x, c, s, acc)
+        torch.cuda.synchronize()
+        kt = np.array([[k[0].elapsed_time(k[1]), k[1].elapsed_time(k[2])] for k in kev])
+    ev[4].record()
+    torch.cuda.synchronize()
+    t = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
+    info = {"nnz": A.nnz, "m": A.m}
+    del A
+    gc.collect()
+    return {"build_ms": t[0], "transpose_ms": t[1], "sens_ms": t[2], "mlem_ms": t[3], "job_ms": sum(t),
+            "kernel_ms": kt, "x": x, **info}
+
+
+def main():
+    args = parse_args()
+    w = workload(args.workload)
+    g = w["geom"]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    n_gpus = max(args.gpus, world)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        vals = []
+        per_step_budget = max(4.0, 90.0 / max(args.steps + args.warmup, 1))
+        for i in range(args.warmup + args.steps):
+            r = cpu_job_rate(w, per_step_budget, threads)
+            if i >= args.warmup:
+                vals.append(r)
+        v = statistics.mean(x["value"] for x in vals)
+        base = vals[-1]
+        out = {"metric": metric_name(w), "value": v, "unit": "MLEM iterations/s", "n_gpus": n_gpus,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * w["niter"] / v,
+               "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded ray sample of the same geometry)", "config": config_of(w, 1),
+               "impl": "reference",
+               "cpu_baseline": {"value": v, "unit": "MLEM iterations/s", "cores": base["cores"], "kind": base["kind"],
+                                "sample": base["sample"]},
+               "e2e": {"value": v, "unit": "MLEM iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+               "matrix_build_s": statistics.mean(x["matrix_build_s"] for x in vals)}
+        print(json.dumps(out))
+        return
+
+    import torch
+
+    import raptr_b200 as R
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as td
+
+        torch.cuda.set_device(local_rank)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                              device_id=torch.device("cuda", local_rank))
+        dist = td
+    else:
+        torch.cuda.set_device(local_rank)
+    dev = torch.cuda.current_device()
+    ctx = R.Context(g, dev)
+    all_ch = np.arange(g.n_channels, dtype=np.int32)
+    lo = rank * g.n_channels // world
+    hi = (rank + 1) * g.n_channels // world
+    lst = torch.from_numpy(all_ch[lo:hi]).cuda()
+    y_full = synth_measurement(R, torch, ctx, w, lst, dist)
+    y_dev = torch.from_numpy(y_full[lo:hi]).cuda()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        run_job(R, torch, ctx, w, lst, y_dev, dist)
+    sampler = ClockSampler(gpu_id_for(torch, dev))
+    sampler.start()
+    launches0 = R.kernel_launches()
+    barrier()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("raptr_timed_steps")
+    t_start.record()
+    steps = [run_job(R, torch, ctx, w, lst, y_dev, dist) for _ in range(args.steps)]
+    t_end.record()
+    torch.cuda.nvtx.range_pop()
+    barrier()
+    launches = R.kernel_launches() - launches0
+    clocks = sampler.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t)
+    phase = {k: statistics.mean(s[k] for s in steps) for k in ("build_ms", "transpose_ms", "sens_ms", "mlem_ms")}
+    if dist is not None:
+        t = torch.tensor([phase[k] for k in sorted(phase)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        phase = dict(zip(sorted(phase), t.tolist()))
+    ms_per_step = total_ms / args.steps
+    value = w["niter"] / (ms_per_step / 1e3)
+    nnz = steps[-1]["nnz"]
+    m = steps[-1]["m"]
+    if dist is not None:
+        t = torch.tensor([nnz], dtype=torch.int64, device="cuda")
+        dist.all_reduce(t)
+        nnz_total = int(t)
+    else:
+        nnz_total = nnz
+
+    out = {"metric": metric_name(w), "value": value, "unit": "MLEM iterations/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+           "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded phantom, Poisson counts, Philox rays)", "config": config_of(w, world),
+           "matrix_build_s": phase["build_ms"] / 1e3,
+           "phases_ms": {k: round(v, 3) for k, v in phase.items()},
+           "resident_mlem_iters_per_s": w["niter"] / (phase["mlem_ms"] / 1e3),
+           "nnz": nnz_total, "gpu_launches": int(launches), "clocks": clocks}
+
+    if rank == 0:
+        # Roofline of the HBM-bound MLEM passes, from the per-kernel device
+        # times of the timed steps.
+        peak, peak_kind = measured_peaks()
+        kts = np.concatenate([s["kernel_ms"] for s in steps])
+        if np.all(np.isfinite(kts)):
+            fwd_ms, back_ms = float(kts[:, 0].mean()), float(kts[:, 1].mean())
+            n = g.n_voxels
+            fwd_bytes = nnz * 8 + (m + 1) * 8 + m * 4 + m * 4 + n * 4
+            back_bytes = nnz * 8 + (n + 1) * 8 + 3 * n * 4 + m * 4
+            r_f = fwd_bytes / (fwd_ms / 1e3) / 1e9
+            r_b = back_bytes / (back_ms / 1e3) / 1e9
+            dom = ("mlem_back_kernel (column gather + update)", r_b, back_bytes, back_ms) if back_ms >= fwd_ms else \
+                ("mlem_forward_kernel (row SpMV + ratio)", r_f, fwd_bytes, fwd_ms)
+            out["roofline"] = {"bound": "hbm", "kernel": dom[0], "achieved": round(dom[1], 1), "peak": peak,
+                               "unit": "GB/s", "frac": round(dom[1] / peak, 4), "peak_source": peak_kind,
+                               "traffic": None, "algorithmic_bytes": int(dom[2]), "launch_ms": round(dom[3], 4)}
+            out["roofline_all"] = {
+                "mlem_forward_kernel": {"achieved": round(r_f, 1), "frac": round(r_f / peak, 4),
+                                        "bytes": int(fwd_bytes), "ms": round(fwd_ms, 4)},
+                "mlem_back_kernel": {"achieved": round(r_b, 1), "frac": round(r_b / peak, 4),
+                                     "bytes": int(back_bytes), "ms": round(back_ms, 4)},
+            }
+        out["build_throughput"] = {"rays_per_s": g.n_channels * w["nrays"] / (phase["build_ms"] / 1e3),
+                                   "entries_per_s": nnz_total / (phase["build_ms"] / 1e3)}
+
+    # End to end through the public C ABI from host buffers (rank 0, N=1).
+    if not args.no_e2e and world == 1:
+        times, st = [], None
+        for _ in range(max(1, min(args.steps, 2))):
+            t0 = time.perf_counter()
+            x_h, st = R.reco_host(g, y_full, w["nrays"], SEED, w["niter"], device=dev)
+            times.append(time.perf_counter() - t0)
+        e2e_s = statistics.mean(times)
+        out["e2e"] = {"value": w["niter"] / e2e_s, "unit": "MLEM iterations/s",
+                      "h2d_bytes_per_step": int(st["h2d_bytes"]), "d2h_bytes_per_step": int(st["d2h_bytes"]),
+                      "wall_s": e2e_s, "build_ms": st["build_ms"], "iter_ms": st["iter_ms"]}
+    if rank == 0 and world == 1:
+        out["cpu_baseline"] = {k: v for k, v in cpu_job_rate(w, args.cpu_sample_s, os.cpu_count() or 1).items()
+                               if k != "matrix_build_s"}
+    if rank == 0:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -74,6 +74,9 @@ typedef struct raptr_matrix raptr_matrix;
 
 int raptr_abi_version(void);
 const char* raptr_last_error(void);
+/* Number of kernels this library has launched in this process (kernels
+ * replayed from a CUDA graph included). */
+int64_t raptr_kernel_launches(void);
 
 raptr_status raptr_ctx_create(const raptr_geom* geom, int device, raptr_ctx** out);
 raptr_status raptr_ctx_destroy(raptr_ctx* ctx);
@@ -137,7 +140,21 @@ raptr_status raptr_matrix_info(const raptr_matrix* A, int64_t* m, int64_t* n, in
                                int32_t** d_col, float** d_val);
 raptr_status raptr_matrix_destroy(raptr_matrix* A);
 
+/* Transpose (CSC) of the library matrix, built once and kept resident beside
+ * the CSR (same values, grouped by voxel): back projection then gathers by
+ * columns instead of scattering with atomics.  Synchronises the stream. */
+raptr_status raptr_matrix_transpose(raptr_matrix* A, void* stream);
+/* Pointers of the transpose (null until raptr_matrix_transpose). */
+raptr_status raptr_matrix_csc_info(const raptr_matrix* A, int64_t** d_col_ptr, int32_t** d_row_idx, float** d_tval);
+
 /* ---- sparse formats --------------------------------------------------------- */
+
+/* CSC of an m x n CSR matrix into caller buffers: d_col_ptr (n+1 int64),
+ * d_row_idx and d_tval (nnz each).  Within a column the row order is not
+ * specified. */
+raptr_status raptr_csr_transpose(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                                 const float* d_val, int64_t* d_col_ptr, int32_t* d_row_idx, float* d_tval,
+                                 void* stream);
 
 /* Row pointers (m+1 int64) from sorted COO row indices (nnz int32). */
 raptr_status raptr_coo2csr(const int32_t* d_rows, int64_t nnz, int64_t m, int64_t* d_row_ptr, void* stream);
@@ -175,15 +192,24 @@ raptr_status raptr_sensitivity(int64_t m, int64_t n, const int64_t* d_row_ptr, c
 typedef struct raptr_mlem_opts {
   int32_t use_graph;   /* capture the iteration loop in a CUDA graph            */
   double* h_loglik;    /* optional: per-iteration Poisson log-likelihood (FP64)  */
+  float* h_kernel_ms;  /* optional: 2*n_iter device times (ms) of the two passes of
+                          each iteration, from CUDA events on the stream; when
+                          set the loop is launched without a graph             */
 } raptr_mlem_opts;
 
 /* n_iter MLEM iterations in the order of src/tests/reco.cu:230-303:
  * yt = A x; e = y / yt; c = A^T e; x = x*c/(s + (s==0)); x *= 1/sum(x).
- * Rows of A correspond to d_y.  d_s is the normalised sensitivity.  d_x is
- * updated in place.  One fused pass over A per iteration. */
+ * Rows of A correspond to d_y; rows with y == 0 are not measured and are
+ * skipped (the reference's matrix has no such rows).  d_s is the normalised
+ * sensitivity.  d_x is updated in place.  With the transpose given
+ * (d_col_ptr, d_row_idx, d_tval non-null) an iteration is two gather passes
+ * (rows, then columns, with the ratio and the update fused into them);
+ * without it, one pass over the rows that scatters the back projection with
+ * atomics. */
 raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
-                        const float* d_val, const float* d_y, const float* d_s, float* d_x, int32_t n_iter,
-                        const raptr_mlem_opts* opts, void* stream);
+                        const float* d_val, const int64_t* d_col_ptr, const int32_t* d_row_idx, const float* d_tval,
+                        const float* d_y, const float* d_s, float* d_x, int32_t n_iter, const raptr_mlem_opts* opts,
+                        void* stream);
 
 /* The two halves of one MLEM iteration, for callers that combine partial
  * back projections across devices (row-sharded matrix):
@@ -195,6 +221,14 @@ raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_r
 raptr_status raptr_mlem_project(int64_t m, const int64_t* d_row_ptr, const int32_t* d_col, const float* d_val,
                                 const float* d_y, const float* d_x, float* d_c, double* d_ll, void* stream);
 raptr_status raptr_mlem_update(int64_t n, float* d_x, float* d_c, const float* d_s, double* d_acc, void* stream);
+/* The same halves on the row/column pair:
+ *   raptr_mlem_forward: d_e = d_y / (A d_x) over the rows of this shard
+ *     (0 where y == 0), optional FP64 log-likelihood sums into d_ll[0..1];
+ *   raptr_mlem_back: d_c = A^T d_e by columns (this shard's partial sums). */
+raptr_status raptr_mlem_forward(int64_t m, const int64_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                                const float* d_y, const float* d_x, float* d_e, double* d_ll, void* stream);
+raptr_status raptr_mlem_back(int64_t n, const int64_t* d_col_ptr, const int32_t* d_row_idx, const float* d_tval,
+                             const float* d_e, float* d_c, void* stream);
 
 /* ---- end-to-end ------------------------------------------------------------ */
 

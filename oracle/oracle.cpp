@@ -436,6 +436,14 @@ void ora_philox4x32_10(const uint32_t* ctr, const uint32_t* key, uint32_t* out) 
 
 void ora_ray_uniforms(uint32_t seed, int64_t cnl, int64_t ray, float* u) { ray_uniforms(seed, cnl, ray, u); }
 
+/* Unit-cube coordinates of rays [0, nrays) of each listed channel
+ * (n * nrays * 6 floats). */
+void ora_ray_uniforms_batch(uint32_t seed, const int32_t* cnl, int64_t n, int32_t nrays, float* out) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; i++)
+    for (int32_t r = 0; r < nrays; r++) ray_uniforms(seed, cnl[i], r, out + (i * nrays + r) * 6);
+}
+
 void ora_channel_split(const OGeom* g, int64_t cnl, int32_t* out5) {
   ChannelIds c = channel_split(*g, cnl);
   out5[0] = c.ida; out5[1] = c.id0z; out5[2] = c.id0y; out5[3] = c.id1z; out5[4] = c.id1y;

@@ -81,6 +81,7 @@ def lib():
             "ora_abi_version": (C.c_int, []),
             "ora_philox4x32_10": (None, [_u32p, _u32p, _u32p]),
             "ora_ray_uniforms": (None, [C.c_uint32, C.c_int64, C.c_int64, _f32p]),
+            "ora_ray_uniforms_batch": (None, [C.c_uint32, _i32p, C.c_int64, C.c_int32, _f32p]),
             "ora_channel_split": (None, [G, C.c_int64, _i32p]),
             "ora_channel_lin": (C.c_int64, [G, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
             "ora_voxel_split": (None, [G, C.c_int64, _i32p]),
@@ -181,6 +182,13 @@ def ray_uniforms(seed, cnl, ray):
     u = np.zeros(6, np.float32)
     lib().ora_ray_uniforms(seed, cnl, ray, u)
     return u
+
+
+def ray_uniforms_batch(seed, cnl, nrays):
+    cnl = np.ascontiguousarray(cnl, np.int32)
+    out = np.zeros((cnl.size, nrays, 6), np.float32)
+    lib().ora_ray_uniforms_batch(seed, cnl, cnl.size, nrays, out)
+    return out
 
 
 def channel_split(g, cnl):

@@ -54,7 +54,7 @@ class raptr_geom(C.Structure):
 
 
 class raptr_mlem_opts(C.Structure):
-    _fields_ = [("use_graph", C.c_int32), ("h_loglik", C.POINTER(C.c_double))]
+    _fields_ = [("use_graph", C.c_int32), ("h_loglik", C.POINTER(C.c_double)), ("h_kernel_ms", C.POINTER(C.c_float))]
 
 
 class raptr_reco_stats(C.Structure):
@@ -90,6 +90,7 @@ P64 = C.POINTER(C.c_int64)
 _SIGNATURES = {
     "raptr_abi_version": (C.c_int, []),
     "raptr_last_error": (C.c_char_p, []),
+    "raptr_kernel_launches": (I64, []),
     "raptr_ctx_create": (C.c_int, [C.POINTER(raptr_geom), C.c_int, C.POINTER(VP)]),
     "raptr_ctx_destroy": (C.c_int, [VP]),
     "raptr_ctx_num_channels": (I64, [VP]),
@@ -111,7 +112,13 @@ _SIGNATURES = {
     "raptr_sensitivity": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP]),
     "raptr_mlem_project": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_mlem_update": (C.c_int, [I64, VP, VP, VP, VP, VP]),
-    "raptr_mlem": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, I32, C.POINTER(raptr_mlem_opts), VP]),
+    "raptr_mlem": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32, C.POINTER(raptr_mlem_opts),
+                             VP]),
+    "raptr_mlem_forward": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, VP, VP]),
+    "raptr_mlem_back": (C.c_int, [I64, VP, VP, VP, VP, VP, VP]),
+    "raptr_matrix_transpose": (C.c_int, [VP, VP]),
+    "raptr_matrix_csc_info": (C.c_int, [VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP)]),
+    "raptr_csr_transpose": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_reco_host": (C.c_int, [C.POINTER(raptr_geom), C.c_int, VP, I32, C.c_uint32, I32, VP, VP, VP,
                                   C.POINTER(raptr_reco_stats)]),
 }
@@ -193,6 +200,30 @@ class Matrix:
         if h is not None and h.value and _lib is not None:
             _lib.raptr_matrix_destroy(h)
             self._h = VP(0)
+
+    @property
+    def has_transpose(self) -> bool:
+        return self.col_ptr is not None
+
+    col_ptr = None
+    row_idx = None
+    tval = None
+
+    def transpose(self, stream=None) -> "Matrix":
+        """Builds the resident CSC copy used by the gather back projection."""
+        _check(lib().raptr_matrix_transpose(self._h, _stream(stream)))
+        cp, ri, tv = VP(), VP(), VP()
+        _check(lib().raptr_matrix_csc_info(self._h, C.byref(cp), C.byref(ri), C.byref(tv)))
+        torch = _torch()
+        dev = torch.device("cuda", self.device)
+        self.col_ptr = torch.as_tensor(_DeviceArray(cp.value, (self.n + 1,), "<i8", self), device=dev)
+        if self.nnz > 0:
+            self.row_idx = torch.as_tensor(_DeviceArray(ri.value, (self.nnz,), "<i4", self), device=dev)
+            self.tval = torch.as_tensor(_DeviceArray(tv.value, (self.nnz,), "<f4", self), device=dev)
+        else:
+            self.row_idx = torch.zeros(0, dtype=torch.int32, device=dev)
+            self.tval = torch.zeros(0, dtype=torch.float32, device=dev)
+        return self
 
     def to_numpy(self):
         return self.row_ptr.cpu().numpy(), self.col.cpu().numpy(), self.val.cpu().numpy()
@@ -285,13 +316,24 @@ class Context:
             _check(st)
         return st, nnz.value
 
-    def mlem(self, A: Matrix, y, s, x, niter: int, use_graph: bool = True, loglik: bool = False, stream=None):
-        """MLEM iterations in place on x; returns per-iteration log-likelihood or None."""
+    def mlem(self, A: Matrix, y, s, x, niter: int, use_graph: bool = True, loglik: bool = False,
+             kernel_times: bool = False, stream=None):
+        """MLEM iterations in place on x.  Returns the per-iteration
+        log-likelihood (loglik) and/or the (n_iter, 2) device times in ms of
+        the two passes of each iteration (kernel_times), else None."""
         ll = (C.c_double * max(niter, 1))() if loglik else None
-        opts = raptr_mlem_opts(1 if use_graph else 0, C.cast(ll, C.POINTER(C.c_double)) if loglik else None)
-        _check(lib().raptr_mlem(self._h, A.m, A.n, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(y), _ptr(s),
-                                _ptr(x), niter, C.byref(opts), _stream(stream)))
-        return np.array(ll[:niter]) if loglik else None
+        kt = (C.c_float * max(2 * niter, 1))() if kernel_times else None
+        opts = raptr_mlem_opts(1 if use_graph else 0, C.cast(ll, C.POINTER(C.c_double)) if loglik else None,
+                               C.cast(kt, C.POINTER(C.c_float)) if kernel_times else None)
+        _check(lib().raptr_mlem(self._h, A.m, A.n, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(A.col_ptr),
+                                _ptr(A.row_idx), _ptr(A.tval), _ptr(y), _ptr(s), _ptr(x), niter, C.byref(opts),
+                                _stream(stream)))
+        out = []
+        if loglik:
+            out.append(np.array(ll[:niter]))
+        if kernel_times:
+            out.append(np.array(kt[:2 * niter], np.float64).reshape(niter, 2))
+        return None if not out else (out[0] if len(out) == 1 else tuple(out))
 
 
 # -- context-free operations ---------------------------------------------------
@@ -319,6 +361,27 @@ def sensitivity(A: Matrix, stream=None):
 def mlem_project(A: Matrix, y, x, c, ll=None, stream=None):
     _check(lib().raptr_mlem_project(A.m, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(y), _ptr(x), _ptr(c),
                                     _ptr(ll), _stream(stream)))
+
+
+def mlem_forward(A: Matrix, y, x, e, ll=None, stream=None):
+    _check(lib().raptr_mlem_forward(A.m, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(y), _ptr(x), _ptr(e),
+                                    _ptr(ll), _stream(stream)))
+
+
+def mlem_back(A: Matrix, e, c, stream=None):
+    assert A.has_transpose, "call A.transpose() first"
+    _check(lib().raptr_mlem_back(A.n, _ptr(A.col_ptr), _ptr(A.row_idx), _ptr(A.tval), _ptr(e), _ptr(c),
+                                 _stream(stream)))
+
+
+def csr_transpose(m: int, n: int, row_ptr, col, val, stream=None):
+    torch = _torch()
+    cp = torch.empty(n + 1, dtype=torch.int64, device=row_ptr.device)
+    ri = torch.empty(max(col.numel(), 1), dtype=torch.int32, device=row_ptr.device)
+    tv = torch.empty(max(col.numel(), 1), dtype=torch.float32, device=row_ptr.device)
+    _check(lib().raptr_csr_transpose(m, n, _ptr(row_ptr), _ptr(col), _ptr(val), _ptr(cp), _ptr(ri), _ptr(tv),
+                                     _stream(stream)))
+    return cp, ri[:col.numel()], tv[:col.numel()]
 
 
 def mlem_update(x, c, s, acc, stream=None):
@@ -357,6 +420,11 @@ def csr2ecsr(yrow, csr, stream=None):
     return out
 
 
+def kernel_launches() -> int:
+    """Kernels launched by the library in this process so far."""
+    return lib().raptr_kernel_launches()
+
+
 def reco_host(geom: Geometry, y: np.ndarray, nrays: int, seed: int, niter: int, sens: Optional[np.ndarray] = None,
               x0: Optional[np.ndarray] = None, device: int = 0):
     """The reco flow from host arrays: returns (x, stats dict)."""
@@ -376,6 +444,6 @@ def reco_host(geom: Geometry, y: np.ndarray, nrays: int, seed: int, niter: int, 
 
 __all__ = [
     "Geometry", "SMALL", "FULL", "FINE", "WORKLOADS", "epet_geometry", "phantom", "poisson_measurement", "Context",
-    "Matrix", "spmv", "sensitivity", "mlem_project", "mlem_update", "divides", "divides_multiplies", "scales",
+    "Matrix", "spmv", "sensitivity", "mlem_project", "mlem_forward", "mlem_back", "csr_transpose", "mlem_update", "divides", "divides_multiplies", "scales",
     "vsum", "coo2csr", "csr2ecsr", "reco_host", "lib", "RaptrError", "OP_N", "OP_T",
 ]

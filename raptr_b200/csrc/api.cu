@@ -133,6 +133,10 @@ struct raptr_matrix {
   int64_t* rp = nullptr;
   int32_t* col = nullptr;
   float* val = nullptr;
+  // transpose (CSC), built on request
+  int64_t* cp = nullptr;
+  int32_t* trow = nullptr;
+  float* tval = nullptr;
 };
 
 namespace {
@@ -297,6 +301,8 @@ extern "C" {
 int raptr_abi_version(void) { return RAPTR_ABI_VERSION; }
 
 const char* raptr_last_error(void) { return g_last_error.c_str(); }
+
+int64_t raptr_kernel_launches(void) { return launches_so_far(); }
 
 raptr_status raptr_ctx_create(const raptr_geom* geom, int device, raptr_ctx** out) {
   if (!out) return fail(RAPTR_ERR_INVALID, "out is null");
@@ -490,7 +496,75 @@ raptr_status raptr_matrix_destroy(raptr_matrix* A) {
   cudaFree(A->rp);
   cudaFree(A->col);
   cudaFree(A->val);
+  cudaFree(A->cp);
+  cudaFree(A->trow);
+  cudaFree(A->tval);
   delete A;
+  return RAPTR_OK;
+}
+
+raptr_status raptr_csr_transpose(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                                 const float* d_val, int64_t* d_col_ptr, int32_t* d_row_idx, float* d_tval,
+                                 void* stream) {
+  if (m < 0 || n <= 0 || !d_row_ptr || !d_col_ptr) return fail(RAPTR_ERR_INVALID, "bad argument");
+  cudaStream_t s = as_stream(stream);
+  int64_t nnz = 0;
+  RCU(cudaMemcpyAsync(&nnz, d_row_ptr + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  RCU(cudaStreamSynchronize(s));
+  if (nnz > 0 && (!d_col || !d_val || !d_row_idx || !d_tval)) return fail(RAPTR_ERR_INVALID, "null buffer");
+  int32_t* cnt = nullptr;
+  int64_t *wide = nullptr, *tmp = nullptr;
+  RCU(cudaMallocAsync(&cnt, size_t(n) * sizeof(int32_t), s));
+  cudaError_t e = cudaMallocAsync(&wide, size_t(n) * sizeof(int64_t), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&tmp, size_t(scan_temp_elems(n)) * sizeof(int64_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, size_t(n) * sizeof(int32_t), s);
+  if (e == cudaSuccess) e = launch_column_counts(nnz, d_col, cnt, s);
+  if (e == cudaSuccess) e = launch_widen(n, cnt, wide, s);
+  if (e == cudaSuccess) e = launch_scan_i64(wide, n, d_col_ptr, tmp, s);
+  // cursors start at the column pointers
+  if (e == cudaSuccess) e = cudaMemcpyAsync(wide, d_col_ptr, size_t(n) * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = launch_transpose_fill(m, d_row_ptr, d_col, d_val, wide, d_row_idx, d_tval, s);
+  if (cnt) cudaFreeAsync(cnt, s);
+  if (wide) cudaFreeAsync(wide, s);
+  if (tmp) cudaFreeAsync(tmp, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "raptr_csr_transpose");
+  return RAPTR_OK;
+}
+
+raptr_status raptr_matrix_transpose(raptr_matrix* A, void* stream) {
+  if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
+  if (A->cp) return RAPTR_OK;
+  DeviceScope ds(A->device);
+  RCU(cudaMalloc(&A->cp, size_t(A->n + 1) * sizeof(int64_t)));
+  cudaError_t e = cudaMalloc(&A->trow, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&A->tval, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(float));
+  if (e != cudaSuccess) {
+    cudaFree(A->cp);
+    cudaFree(A->trow);
+    cudaFree(A->tval);
+    A->cp = nullptr;
+    A->trow = nullptr;
+    A->tval = nullptr;
+    return cuda_fail(e, "cudaMalloc(transpose)");
+  }
+  raptr_status st = raptr_csr_transpose(A->m, A->n, A->rp, A->col, A->val, A->cp, A->trow, A->tval, stream);
+  if (st != RAPTR_OK) {
+    cudaFree(A->cp);
+    cudaFree(A->trow);
+    cudaFree(A->tval);
+    A->cp = nullptr;
+    A->trow = nullptr;
+    A->tval = nullptr;
+  }
+  return st;
+}
+
+raptr_status raptr_matrix_csc_info(const raptr_matrix* A, int64_t** d_col_ptr, int32_t** d_row_idx, float** d_tval) {
+  if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
+  if (d_col_ptr) *d_col_ptr = A->cp;
+  if (d_row_idx) *d_row_idx = A->trow;
+  if (d_tval) *d_tval = A->tval;
   return RAPTR_OK;
 }
 
@@ -588,19 +662,44 @@ raptr_status raptr_mlem_update(int64_t n, float* d_x, float* d_c, const float* d
   return RAPTR_OK;
 }
 
+raptr_status raptr_mlem_forward(int64_t m, const int64_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                                const float* d_y, const float* d_x, float* d_e, double* d_ll, void* stream) {
+  if (m < 0 || !d_row_ptr || !d_y || !d_x || !d_e) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, d_e, d_ll, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_mlem_back(int64_t n, const int64_t* d_col_ptr, const int32_t* d_row_idx, const float* d_tval,
+                             const float* d_e, float* d_c, void* stream) {
+  if (n <= 0 || !d_col_ptr || !d_e || !d_c) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_mlem_back(n, d_col_ptr, d_row_idx, d_tval, d_e, nullptr, nullptr, d_c, nullptr, false,
+                       as_stream(stream)));
+  return RAPTR_OK;
+}
+
 raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
-                        const float* d_val, const float* d_y, const float* d_s, float* d_x, int32_t n_iter,
-                        const raptr_mlem_opts* opts, void* stream) {
+                        const float* d_val, const int64_t* d_col_ptr, const int32_t* d_row_idx, const float* d_tval,
+                        const float* d_y, const float* d_s, float* d_x, int32_t n_iter, const raptr_mlem_opts* opts,
+                        void* stream) {
   if (!ctx || m < 0 || n <= 0 || n_iter < 0 || !d_row_ptr || !d_y || !d_s || !d_x)
     return fail(RAPTR_ERR_INVALID, "bad argument");
   if (n_iter == 0) return RAPTR_OK;
   DeviceScope ds(ctx->device);
   cudaStream_t s = as_stream(stream);
   const bool want_ll = opts && opts->h_loglik;
-  const bool use_graph = opts && opts->use_graph;
-  RCHECK(ctx->ensure_scratch(Carve::need({size_t(n) * sizeof(float), size_t(2 * n_iter + 2) * sizeof(double)})));
+  const bool want_times = opts && opts->h_kernel_ms;
+  const bool use_graph = opts && opts->use_graph && !want_times;
+  const bool csc = d_col_ptr != nullptr;
+  std::vector<cudaEvent_t> evs;
+  if (want_times) {
+    evs.resize(size_t(3 * n_iter));
+    for (auto& ev : evs) RCU(cudaEventCreate(&ev));
+  }
+  RCHECK(ctx->ensure_scratch(Carve::need({size_t(n) * sizeof(float), size_t(csc ? m : 1) * sizeof(float),
+                                          size_t(2 * n_iter + 2) * sizeof(double)})));
   Carve cv(ctx->d_scratch);
-  float* c = cv.take<float>(size_t(n));
+  float* c = cv.take<float>(size_t(n));  // correction (scatter path) or x before normalisation
+  float* e = cv.take<float>(size_t(csc ? m : 1));
   double* acc = cv.take<double>(size_t(2 * n_iter + 2));
   double* ll = acc + 2;
   RCU(cudaMemsetAsync(c, 0, size_t(n) * sizeof(float), s));
@@ -608,11 +707,23 @@ raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_r
 
   auto enqueue = [&](cudaStream_t q) -> cudaError_t {
     for (int32_t it = 0; it < n_iter; it++) {
-      cudaError_t e = launch_mlem_project(m, d_row_ptr, d_col, d_val, d_y, d_x, c, want_ll ? ll + 2 * it : nullptr, q);
-      if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, sizeof(double), q);
-      if (e == cudaSuccess) e = launch_mlem_update(n, d_x, c, d_s, acc, q);
-      if (e == cudaSuccess) e = launch_mlem_normalise(n, d_x, c, acc, q);
-      if (e != cudaSuccess) return e;
+      double* lli = want_ll ? ll + 2 * it : nullptr;
+      cudaError_t err = cudaMemsetAsync(acc, 0, sizeof(double), q);
+      if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it)], q);
+      if (csc) {
+        if (err == cudaSuccess) err = launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, e, lli, q);
+        if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 1)], q);
+        if (err == cudaSuccess) err = launch_mlem_back(n, d_col_ptr, d_row_idx, d_tval, e, d_x, d_s, c, acc, true, q);
+        if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 2)], q);
+        if (err == cudaSuccess) err = launch_mlem_normalise_from(n, d_x, c, acc, q);
+      } else {
+        if (err == cudaSuccess) err = launch_mlem_project(m, d_row_ptr, d_col, d_val, d_y, d_x, c, lli, q);
+        if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 1)], q);
+        if (err == cudaSuccess) err = launch_mlem_update(n, d_x, c, d_s, acc, q);
+        if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 2)], q);
+        if (err == cudaSuccess) err = launch_mlem_normalise(n, d_x, c, acc, q);
+      }
+      if (err != cudaSuccess) return err;
     }
     return cudaSuccess;
   };
@@ -636,6 +747,9 @@ raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_r
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (e == cudaSuccess) e = cudaGraphLaunch(exec, cap);
+    // the captured launches were counted once at capture; replaying the
+    // graph launches them again
+    if (e == cudaSuccess) note_launches(3LL * n_iter);
     if (e == cudaSuccess) e = cudaEventRecord(ev, cap);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cap);
@@ -644,6 +758,17 @@ raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_r
     cudaEventDestroy(ev);
     cudaStreamDestroy(cap);
     if (e != cudaSuccess) return cuda_fail(e, "MLEM graph");
+  }
+  if (want_times) {
+    RCU(cudaStreamSynchronize(s));
+    for (int32_t it = 0; it < n_iter; it++) {
+      float a = 0.f, b = 0.f;
+      RCU(cudaEventElapsedTime(&a, evs[size_t(3 * it)], evs[size_t(3 * it + 1)]));
+      RCU(cudaEventElapsedTime(&b, evs[size_t(3 * it + 1)], evs[size_t(3 * it + 2)]));
+      opts->h_kernel_ms[2 * it] = a;
+      opts->h_kernel_ms[2 * it + 1] = b;
+    }
+    for (auto& ev : evs) cudaEventDestroy(ev);
   }
   if (want_ll) {
     std::vector<double> h(size_t(2 * n_iter));
@@ -716,6 +841,12 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
     cleanup();
     return fail(st, msg);
   }
+  st = raptr_matrix_transpose(A, s);
+  if (st != RAPTR_OK) {
+    std::string msg = g_last_error;
+    cleanup();
+    return fail(st, msg);
+  }
   RSTEP(cudaEventRecord(ev[2], s));
   if (!h_sens) {
     RSTEP(cudaMalloc(&d_s64, size_t(N) * sizeof(double)));
@@ -746,8 +877,8 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
     h2d += N * int64_t(sizeof(float));
   }
   RSTEP(cudaEventRecord(ev[3], s));
-  raptr_mlem_opts o{1, nullptr};
-  st = raptr_mlem(ctx, A->m, N, A->rp, A->col, A->val, d_y, d_s, d_x, n_iter, &o, s);
+  raptr_mlem_opts o{1, nullptr, nullptr};
+  st = raptr_mlem(ctx, A->m, N, A->rp, A->col, A->val, A->cp, A->trow, A->tval, d_y, d_s, d_x, n_iter, &o, s);
   if (st != RAPTR_OK) {
     std::string msg = g_last_error;
     cleanup();

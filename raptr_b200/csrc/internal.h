@@ -9,6 +9,10 @@
 
 namespace raptr {
 
+// Process-wide count of kernels launched by this library (diagnostic).
+void note_launches(long long k);
+long long launches_so_far();
+
 // ---- system matrix rows (kernels_sm.cu) ----------------------------------
 
 // Hash/slot capacity levels for the per-channel accumulation table; a row
@@ -92,7 +96,22 @@ cudaError_t launch_mlem_project(int64_t m, const int64_t* rp, const int32_t* col
 cudaError_t launch_mlem_update(int64_t n, float* x, const float* c, const float* sens, double* d_acc, cudaStream_t s);
 // x *= float(1/float(d_acc[0])); c = 0; d_acc[0] reset by the next project.
 cudaError_t launch_mlem_normalise(int64_t n, float* x, float* c, double* d_acc, cudaStream_t s);
+cudaError_t launch_mlem_normalise_from(int64_t n, float* x, const float* xx, double* d_acc, cudaStream_t s);
 cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s);
+
+// Transpose (CSC) of a CSR matrix: column counts (int32 atomics), widening to
+// int64, and the fill through per-column cursors (initialised to col_ptr).
+cudaError_t launch_column_counts(int64_t nnz, const int32_t* col, int32_t* cnt, cudaStream_t s);
+cudaError_t launch_widen(int64_t n, const int32_t* a, int64_t* b, cudaStream_t s);
+cudaError_t launch_transpose_fill(int64_t m, const int64_t* rp, const int32_t* col, const float* val,
+                                  int64_t* cursor, int32_t* trow, float* tval, cudaStream_t s);
+// e_i = y_i / (A x)_i (0 for y_i == 0); optional FP64 log-likelihood sums.
+cudaError_t launch_mlem_forward(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const float* y,
+                                const float* x, float* e, double* d_ll, cudaStream_t s);
+// c_j = (A^T e)_j by columns; with update: out = x*c/(s+(s==0)), d_acc += sum.
+cudaError_t launch_mlem_back(int64_t n, const int64_t* cp, const int32_t* trow, const float* tval, const float* e,
+                             const float* x, const float* sens, float* out, double* d_acc, bool update,
+                             cudaStream_t s);
 cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s);
 
 }  // namespace raptr

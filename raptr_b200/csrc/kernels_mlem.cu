@@ -237,14 +237,113 @@ __global__ void __launch_bounds__(kThreads) mlem_update_kernel(int64_t n, float*
   block_add_double(sum, acc);
 }
 
-__global__ void mlem_normalise_kernel(int64_t n, float* __restrict__ x, float* __restrict__ c,
-                                      const double* __restrict__ acc) {
+// x = scale * xx with scale = float(1/float(sum)) as src/tests/reco.cu:300-302
+// (norm = sum(x); scales(x, val_t(1./norm))); clears c when given.
+__global__ void mlem_normalise_kernel(int64_t n, float* __restrict__ x, const float* __restrict__ xx,
+                                      float* __restrict__ c, const double* __restrict__ acc) {
   const float norm = float(*acc);
   const float scale = float(1.0 / double(norm));
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    x[i] = __fmul_rn(scale, x[i]);
-    c[i] = 0.f;
+    x[i] = __fmul_rn(scale, xx[i]);
+    if (c) c[i] = 0.f;
   }
+}
+
+// ---- transpose (CSC) and the two-pass MLEM iteration ------------------------
+
+__global__ void colcount_kernel(int64_t nnz, const int32_t* __restrict__ col, int32_t* __restrict__ cnt) {
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < nnz; k += int64_t(gridDim.x) * blockDim.x)
+    atomicAdd(cnt + __ldcs(col + k), 1);
+}
+
+__global__ void widen_kernel(int64_t n, const int32_t* __restrict__ a, int64_t* __restrict__ b) {
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+    b[k] = a[k];
+}
+
+// Places entry (r, j) of the CSR matrix at the next free slot of column j.
+__global__ void __launch_bounds__(kThreads) transpose_fill_kernel(int64_t m, const int64_t* __restrict__ rp,
+                                                                  const int32_t* __restrict__ col,
+                                                                  const float* __restrict__ val,
+                                                                  unsigned long long* __restrict__ cursor,
+                                                                  int32_t* __restrict__ trow,
+                                                                  float* __restrict__ tval) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+    const int64_t b = rp[r], e = rp[r + 1];
+    for (int64_t k = b + lane; k < e; k += 32) {
+      const int j = __ldcs(col + k);
+      const unsigned long long p = atomicAdd(cursor + j, 1ull);
+      trow[p] = int32_t(r);
+      tval[p] = __ldcs(val + k);
+    }
+  }
+}
+
+// Forward projection with the ratio: e_i = y_i / <a_i, x> for measured rows
+// (y_i != 0), e_i = 0 otherwise.
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads) mlem_forward_kernel(int64_t m, const int64_t* __restrict__ rp,
+                                                                const int32_t* __restrict__ col,
+                                                                const float* __restrict__ val,
+                                                                const float* __restrict__ y,
+                                                                const float* __restrict__ x, float* __restrict__ e,
+                                                                double* __restrict__ ll) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  double ly = 0.0, lt = 0.0;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+    const float yi = __ldg(y + r);
+    if (yi == 0.f) {
+      if (lane == 0) e[r] = 0.f;
+      continue;
+    }
+    const float yt = row_dot<VEC>(col, val, rp[r], rp[r + 1], x, lane);
+    if (lane == 0) {
+      e[r] = __fdiv_rn(yi, yt);
+      if (ll) {
+        ly += double(yi) * log(double(yt));
+        lt += double(yt);
+      }
+    }
+  }
+  if (ll) {
+    block_add_double(ly, ll);
+    __syncthreads();
+    block_add_double(lt, ll + 1);
+  }
+}
+
+// Back projection by columns: c_j = <column j of A, e>.  With UPDATE the
+// MLEM update follows in the epilogue: xx_j = x_j*c_j/(s_j + (s_j==0)) and
+// acc += sum xx (FP64); without it c_j is stored.
+template <bool VEC, bool UPDATE>
+__global__ void __launch_bounds__(kThreads) mlem_back_kernel(int64_t n, const int64_t* __restrict__ cp,
+                                                             const int32_t* __restrict__ trow,
+                                                             const float* __restrict__ tval,
+                                                             const float* __restrict__ e,
+                                                             const float* __restrict__ x,
+                                                             const float* __restrict__ sens, float* __restrict__ out,
+                                                             double* __restrict__ acc) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  double sum = 0.0;
+  for (int64_t j = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; j < n; j += nw) {
+    const float c = row_dot<VEC>(trow, tval, cp[j], cp[j + 1], e, lane);
+    if (lane == 0) {
+      if (UPDATE) {
+        float dvs = sens[j];
+        dvs += float(dvs == 0.f);
+        const float xx = __fdiv_rn(__fmul_rn(x[j], c), dvs);
+        out[j] = xx;
+        sum += double(xx);
+      } else {
+        out[j] = c;
+      }
+    }
+  }
+  if (UPDATE) block_add_double(sum, acc);
 }
 
 // The 16-byte vector path needs 16-byte aligned column and value arrays.
@@ -272,76 +371,199 @@ cudaError_t launch_spmv(int op, int64_t m, int64_t n, const int64_t* rp, const i
                         float alpha, const float* x, float beta, float* y, cudaStream_t s) {
   if (op == RAPTR_OP_N) {
     if (m > 0) {
-      if (aligned16(col, val)) spmv_n_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, beta, y);
-      else spmv_n_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, beta, y);
+      if (aligned16(col, val)) {
+        spmv_n_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, beta, y);
+        note_launches(1);
+      }
+      else {
+        spmv_n_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, beta, y);
+        note_launches(1);
+      }
     }
   } else {
-    if (beta != 1.f && n > 0) scale_kernel<<<ew_grid(n), kThreads, 0, s>>>(y, beta, n);
+    if (beta != 1.f && n > 0) {
+      scale_kernel<<<ew_grid(n), kThreads, 0, s>>>(y, beta, n);
+      note_launches(1);
+    }
     if (m > 0) {
-      if (aligned16(col, val)) spmv_t_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, y);
-      else spmv_t_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, y);
+      if (aligned16(col, val)) {
+        spmv_t_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, y);
+        note_launches(1);
+      }
+      else {
+        spmv_t_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, y);
+        note_launches(1);
+      }
     }
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_divides(float* r, const float* a, const float* b, int64_t n, cudaStream_t s) {
-  if (n > 0) divides_kernel<<<ew_grid(n), kThreads, 0, s>>>(r, a, b, n);
+  if (n > 0) {
+    divides_kernel<<<ew_grid(n), kThreads, 0, s>>>(r, a, b, n);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_divides_multiplies(float* r, const float* a, const float* b, const float* c, int64_t n,
                                       cudaStream_t s) {
-  if (n > 0) divmul_kernel<<<ew_grid(n), kThreads, 0, s>>>(r, a, b, c, n);
+  if (n > 0) {
+    divmul_kernel<<<ew_grid(n), kThreads, 0, s>>>(r, a, b, c, n);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_scales(float* x, float alpha, int64_t n, cudaStream_t s) {
-  if (n > 0) scales_kernel<<<ew_grid(n), kThreads, 0, s>>>(x, alpha, n);
+  if (n > 0) {
+    scales_kernel<<<ew_grid(n), kThreads, 0, s>>>(x, alpha, n);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_sum(const float* x, int64_t n, double* d_acc, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(d_acc, 0, sizeof(double), s);
   if (e != cudaSuccess) return e;
-  if (n > 0) sum_kernel<<<ew_grid(n), kThreads, 0, s>>>(x, n, d_acc);
+  if (n > 0) {
+    sum_kernel<<<ew_grid(n), kThreads, 0, s>>>(x, n, d_acc);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_sum_f64(const double* x, int64_t n, double* d_acc, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(d_acc, 0, sizeof(double), s);
   if (e != cudaSuccess) return e;
-  if (n > 0) sum_f64_kernel<<<ew_grid(n), kThreads, 0, s>>>(x, n, d_acc);
+  if (n > 0) {
+    sum_f64_kernel<<<ew_grid(n), kThreads, 0, s>>>(x, n, d_acc);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_column_sums(int64_t m, const int64_t* rp, const int32_t* col, const float* val, double* s64,
                                cudaStream_t s) {
-  if (m > 0) colsum_kernel<<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, s64);
+  if (m > 0) {
+    colsum_kernel<<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, s64);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_sens_normalise(int64_t n, const double* s64, const double* d_total, float* s32, cudaStream_t s) {
-  if (n > 0) sens_norm_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, s64, d_total, s32);
+  if (n > 0) {
+    sens_norm_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, s64, d_total, s32);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_mlem_project(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const float* y,
                                 const float* x, float* c, double* d_ll, cudaStream_t s) {
   if (m > 0) {
-    if (aligned16(col, val)) mlem_project_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, c, d_ll);
-    else mlem_project_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, c, d_ll);
+    if (aligned16(col, val)) {
+      mlem_project_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, c, d_ll);
+      note_launches(1);
+    }
+    else {
+      mlem_project_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, c, d_ll);
+      note_launches(1);
+    }
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_mlem_update(int64_t n, float* x, const float* c, const float* sens, double* d_acc, cudaStream_t s) {
-  if (n > 0) mlem_update_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, x, c, sens, d_acc);
+  if (n > 0) {
+    mlem_update_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, x, c, sens, d_acc);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_mlem_normalise(int64_t n, float* x, float* c, double* d_acc, cudaStream_t s) {
-  if (n > 0) mlem_normalise_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, x, c, d_acc);
+  if (n > 0) {
+    mlem_normalise_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, x, x, c, d_acc);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlem_normalise_from(int64_t n, float* x, const float* xx, double* d_acc, cudaStream_t s) {
+  if (n > 0) {
+    mlem_normalise_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, x, xx, nullptr, d_acc);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_column_counts(int64_t nnz, const int32_t* col, int32_t* cnt, cudaStream_t s) {
+  if (nnz > 0) {
+    colcount_kernel<<<148 * 16, kThreads, 0, s>>>(nnz, col, cnt);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_widen(int64_t n, const int32_t* a, int64_t* b, cudaStream_t s) {
+  if (n > 0) {
+    widen_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, a, b);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_fill(int64_t m, const int64_t* rp, const int32_t* col, const float* val,
+                                  int64_t* cursor, int32_t* trow, float* tval, cudaStream_t s) {
+  if (m > 0)
+    transpose_fill_kernel<<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val,
+                                                           reinterpret_cast<unsigned long long*>(cursor), trow, tval);
+    note_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlem_forward(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const float* y,
+                                const float* x, float* e, double* d_ll, cudaStream_t s) {
+  if (m > 0) {
+    if (aligned16(col, val)) {
+      mlem_forward_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, e, d_ll);
+      note_launches(1);
+    }
+    else {
+      mlem_forward_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, e, d_ll);
+      note_launches(1);
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlem_back(int64_t n, const int64_t* cp, const int32_t* trow, const float* tval, const float* e,
+                             const float* x, const float* sens, float* out, double* d_acc, bool update,
+                             cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const bool v = aligned16(trow, tval);
+  if (update) {
+    if (v) {
+      mlem_back_kernel<true, true><<<row_grid(n), kThreads, 0, s>>>(n, cp, trow, tval, e, x, sens, out, d_acc);
+      note_launches(1);
+    }
+    else {
+      mlem_back_kernel<false, true><<<row_grid(n), kThreads, 0, s>>>(n, cp, trow, tval, e, x, sens, out, d_acc);
+      note_launches(1);
+    }
+  } else {
+    if (v) {
+      mlem_back_kernel<true, false><<<row_grid(n), kThreads, 0, s>>>(n, cp, trow, tval, e, x, sens, out, d_acc);
+      note_launches(1);
+    }
+    else {
+      mlem_back_kernel<false, false><<<row_grid(n), kThreads, 0, s>>>(n, cp, trow, tval, e, x, sens, out, d_acc);
+      note_launches(1);
+    }
+  }
   return cudaGetLastError();
 }
 

@@ -344,6 +344,7 @@ cudaError_t launch_level(const DGeom& g, const float2* d_sincos, const int32_t* 
   if (e != cudaSuccess) return e;
   sm_rows_kernel<H, T><<<unsigned(nrows), T, smem, s>>>(g, d_sincos, d_cnl, row0, nrays, seed, d_rays, st_col,
                                                          st_val, row_nnz, d_flags);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -601,11 +602,13 @@ cudaError_t launch_sm_rows(int level, const DGeom& g, const float2* d_sincos, co
 
 cudaError_t launch_rows_scan(const int32_t* row_nnz, int64_t n, int64_t* row_ptr, int64_t* d_base, cudaStream_t s) {
   rows_scan_kernel<int32_t><<<1, 1024, 0, s>>>(row_nnz, n, row_ptr, d_base);
+  note_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_rows_scan_i64(const int64_t* counts, int64_t n, int64_t* row_ptr, int64_t* d_base, cudaStream_t s) {
   rows_scan_kernel<int64_t><<<1, 1024, 0, s>>>(counts, n, row_ptr, d_base);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -615,6 +618,7 @@ cudaError_t launch_rows_gather(const int32_t* st_col, const float* st_val, int s
   int64_t blocks = (nrows * 32 + 255) / 256;
   if (blocks > 148 * 64) blocks = 148 * 64;
   rows_gather_kernel<<<unsigned(blocks), 256, 0, s>>>(st_col, st_val, slot_cap, row_ptr, nrows, capacity, col, val);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -626,6 +630,7 @@ cudaError_t launch_expand_candidates(const int32_t* st_col, const float* st_val,
   if (blocks > 148 * 64) blocks = 148 * 64;
   expand_kernel<<<unsigned(blocks), 256, 0, s>>>(st_col, st_val, slot_cap, row_nnz, cand_ptr, nrows, cand_vxl,
                                                   out_val);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -633,6 +638,7 @@ cudaError_t launch_rays(const DGeom& g, const float2* d_sincos, const int32_t* d
                         uint32_t seed, float* d_rays, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   rays_kernel<<<unsigned(n), 128, 0, s>>>(g, d_sincos, d_cnl, nrays, seed, d_rays);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -642,6 +648,7 @@ cudaError_t launch_wq_count(const DGeom& g, const float2* d_sincos, const int32_
   if (g.n[1] > kWqMaxNy) return cudaErrorInvalidValue;
   wq_kernel<false><<<unsigned(n), kWqThreads, 0, s>>>(g, d_sincos, d_list, li0, start_vxl, d_counts, nullptr, 0,
                                                       nullptr, nullptr, d_flags);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -652,6 +659,7 @@ cudaError_t launch_wq_fill(const DGeom& g, const float2* d_sincos, const int32_t
   if (g.n[1] > kWqMaxNy) return cudaErrorInvalidValue;
   wq_kernel<true><<<unsigned(n), kWqThreads, 0, s>>>(g, d_sincos, d_list, li0, start_vxl, nullptr, d_offsets,
                                                      max_out, d_cnl_out, d_vxl_out, d_flags);
+  note_launches(1);
   return cudaGetLastError();
 }
 

@@ -1,9 +1,17 @@
 // Device-wide scan and sparse-format utilities.
+#include <atomic>
 #include <cstdint>
 
 #include "internal.h"
 
 namespace raptr {
+
+namespace {
+std::atomic<long long> g_launches{0};
+}
+
+void note_launches(long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 namespace {
 
@@ -125,7 +133,10 @@ unsigned grid_for(int64_t n, int threads) {
 }  // namespace
 
 cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s) {
-  if (n > 0) iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, n);
+  if (n > 0) {
+    iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, n);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
@@ -137,19 +148,24 @@ cudaError_t launch_scan_i64(const int64_t* in, int64_t n, int64_t* out, int64_t*
     return cudaMemsetAsync(out, 0, sizeof(int64_t), s);
   }
   scan_partials<<<unsigned(nb), kScanThreads, 0, s>>>(in, n, temp);
+  note_launches(1);
   scan_spine<<<1, kScanThreads, 0, s>>>(temp, nb);
+  note_launches(1);
   scan_apply<<<unsigned(nb), kScanThreads, 0, s>>>(in, n, temp, out, nb);
+  note_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_coo2csr(const int32_t* rows, int64_t nnz, int64_t m, int64_t* row_ptr, int64_t*, cudaStream_t s) {
   coo2csr_kernel<<<grid_for(m + 1, 256), 256, 0, s>>>(rows, nnz, m, row_ptr);
+  note_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_csr2ecsr(int64_t* ecsr, const int32_t* yrow, int64_t nnzr, const int64_t* csr, int64_t m,
                             cudaStream_t s) {
   csr2ecsr_kernel<<<grid_for(nnzr + 1, 256), 256, 0, s>>>(ecsr, yrow, nnzr, csr, m);
+  note_launches(1);
   return cudaGetLastError();
 }
 

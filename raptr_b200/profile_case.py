@@ -1,0 +1,43 @@
+"""A small, self-contained case of the hot kernels for `ncu` captures.
+
+    python -m raptr_b200.profile_case [--rows R] [--workload full]
+
+Builds rows [0, R) of the workload's system matrix (one build chunk),
+transposes it and runs three MLEM iterations, so that each hot kernel
+(sm_rows_kernel, mlem_forward_kernel, mlem_back_kernel) launches a few times
+on a matrix larger than L2 but only a few GB on the device.
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--rows", type=int, default=65536)
+    p.add_argument("--workload", default="full")
+    a = p.parse_args()
+    import torch
+
+    import raptr_b200 as R
+    from raptr_b200 import config as cfg
+
+    w = cfg.WORKLOADS[a.workload]
+    g = w["geom"]
+    ctx = R.Context(g, 0)
+    lst = torch.arange(a.rows, dtype=torch.int32, device="cuda")
+    A = ctx.build(lst, w["nrays"], 1251)
+    A.transpose()
+    xt = torch.from_numpy(cfg.phantom(g, w["rods"])).cuda()
+    y = R.spmv(R.OP_N, A.m, A.n, A.row_ptr, A.col, A.val, xt) * 1000.0
+    s64, s = R.sensitivity(A)
+    x = torch.full((A.n,), np.float32(1.0 / A.n), device="cuda")
+    ctx.mlem(A, y, s, x, 3, use_graph=False)
+    torch.cuda.synchronize()
+    print(f"profile case: {A.m} rows, {A.nnz} entries ({A.nnz * 8 / 1e9:.2f} GB CSR), x sum {float(x.sum()):.6f}")
+
+
+if __name__ == "__main__":
+    main()
