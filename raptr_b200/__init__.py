@@ -163,11 +163,24 @@ def _stream(stream=None) -> int:
     return s.cuda_stream
 
 
+class _MatrixHandle:
+    """Owns a raptr_matrix*; destroys it when the last reference goes (the
+    Matrix object and every tensor view hold one)."""
+
+    def __init__(self, handle: int):
+        self.h = VP(handle)
+
+    def __del__(self):
+        if self.h.value and _lib is not None:
+            _lib.raptr_matrix_destroy(self.h)
+            self.h = VP(0)
+
+
 class _DeviceArray:
     """Zero-copy __cuda_array_interface__ view of library-owned memory; keeps
-    its owner alive."""
+    the owning handle alive (and nothing else, so no reference cycle)."""
 
-    def __init__(self, ptr: int, shape, typestr: str, owner):
+    def __init__(self, ptr: int, shape, typestr: str, owner: _MatrixHandle):
         self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, False),
                                          "version": 3, "strides": None}
         self._owner = owner
@@ -175,10 +188,12 @@ class _DeviceArray:
 
 class Matrix:
     """System matrix rows held by the library (CSR: int64 row_ptr, int32 col,
-    float32 val), resident in device memory."""
+    float32 val), resident in device memory.  The device memory is released
+    when the Matrix and all tensor views of it are gone."""
 
     def __init__(self, handle: int, device: int):
-        self._h = VP(handle)
+        self._owner = _MatrixHandle(handle)
+        self._h = self._owner.h
         self.device = device
         m, n, nnz = C.c_int64(), C.c_int64(), C.c_int64()
         rp, col, val = VP(), VP(), VP()
@@ -187,19 +202,14 @@ class Matrix:
         self.m, self.n, self.nnz = m.value, n.value, nnz.value
         torch = _torch()
         dev = torch.device("cuda", device)
-        self.row_ptr = torch.as_tensor(_DeviceArray(rp.value, (self.m + 1,), "<i8", self), device=dev)
+        own = self._owner
+        self.row_ptr = torch.as_tensor(_DeviceArray(rp.value, (self.m + 1,), "<i8", own), device=dev)
         if self.nnz > 0:
-            self.col = torch.as_tensor(_DeviceArray(col.value, (self.nnz,), "<i4", self), device=dev)
-            self.val = torch.as_tensor(_DeviceArray(val.value, (self.nnz,), "<f4", self), device=dev)
+            self.col = torch.as_tensor(_DeviceArray(col.value, (self.nnz,), "<i4", own), device=dev)
+            self.val = torch.as_tensor(_DeviceArray(val.value, (self.nnz,), "<f4", own), device=dev)
         else:
             self.col = torch.zeros(0, dtype=torch.int32, device=dev)
             self.val = torch.zeros(0, dtype=torch.float32, device=dev)
-
-    def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value and _lib is not None:
-            _lib.raptr_matrix_destroy(h)
-            self._h = VP(0)
 
     @property
     def has_transpose(self) -> bool:
@@ -216,10 +226,11 @@ class Matrix:
         _check(lib().raptr_matrix_csc_info(self._h, C.byref(cp), C.byref(ri), C.byref(tv)))
         torch = _torch()
         dev = torch.device("cuda", self.device)
-        self.col_ptr = torch.as_tensor(_DeviceArray(cp.value, (self.n + 1,), "<i8", self), device=dev)
+        own = self._owner
+        self.col_ptr = torch.as_tensor(_DeviceArray(cp.value, (self.n + 1,), "<i8", own), device=dev)
         if self.nnz > 0:
-            self.row_idx = torch.as_tensor(_DeviceArray(ri.value, (self.nnz,), "<i4", self), device=dev)
-            self.tval = torch.as_tensor(_DeviceArray(tv.value, (self.nnz,), "<f4", self), device=dev)
+            self.row_idx = torch.as_tensor(_DeviceArray(ri.value, (self.nnz,), "<i4", own), device=dev)
+            self.tval = torch.as_tensor(_DeviceArray(tv.value, (self.nnz,), "<f4", own), device=dev)
         else:
             self.row_idx = torch.zeros(0, dtype=torch.int32, device=dev)
             self.tval = torch.zeros(0, dtype=torch.float32, device=dev)

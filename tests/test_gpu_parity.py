@@ -414,3 +414,23 @@ def test_full_size_matrix_properties(rlib, oracle, torch, ctx_full):
     assert abs(float(row_sums.double().sum()) - total) <= 1e-5 * total
     s64, s = rlib.sensitivity(A)
     assert abs(float(s64.sum()) - total) <= 1e-9 * total
+
+
+def test_matrix_memory_is_released(rlib, torch, ctx_small):
+    """Device memory of a matrix (and its transpose) is returned once the
+    Matrix and its tensor views are dropped."""
+    lst = np.arange(0, 60000, dtype=np.int32)
+    A = ctx_small.build(lst, 100, SEED)  # warms the context scratch
+    del A
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    A = ctx_small.build(lst, 100, SEED)
+    A.transpose()
+    nbytes = A.nnz * 16
+    col_view = A.col[:10]
+    del A
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] < free0 - nbytes // 2  # the view keeps it alive
+    del col_view
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] > free0 - nbytes // 4
