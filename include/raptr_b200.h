@@ -230,6 +230,24 @@ raptr_status raptr_mlem_forward(int64_t m, const int64_t* d_row_ptr, const int32
 raptr_status raptr_mlem_back(int64_t n, const int64_t* d_col_ptr, const int32_t* d_row_idx, const float* d_tval,
                              const float* d_e, float* d_c, void* stream);
 
+/* MLEM iterations that allocate no device memory.  No counterpart in the
+ * reference (which allocates its buffers itself).  For callers that cannot
+ * allocate where they reconstruct -- e.g. a server that reserves its whole
+ * HBM budget up front, or a pipeline that cannot take the synchronisation a
+ * cudaMalloc/cudaFree brings.  Same iteration as raptr_mlem without a
+ * transpose (one pass over the rows, back projection scattered with
+ * atomics); the caller passes the matrix, y, s and x (updated in place).
+ * The workspace is a fixed device array inside the library, sized for at
+ * most 1,048,576 voxels (4 MiB, held on every GPU that loads the library
+ * until exit); larger n is rejected with RAPTR_ERR_INVALID.  Runs on the
+ * current device; the first call on a device looks up the array's device
+ * address, so make that first call before any stream capture.  All calls on
+ * a device share the array: each call clears what must start at zero, and
+ * calls that overlap on the GPU race on it. */
+raptr_status raptr_mlem_noalloc(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                                const float* d_val, const float* d_y, const float* d_s, float* d_x, int32_t n_iter,
+                                void* stream);
+
 /* ---- end-to-end ------------------------------------------------------------ */
 
 typedef struct raptr_reco_stats {

@@ -119,6 +119,7 @@ _SIGNATURES = {
     "raptr_matrix_transpose": (C.c_int, [VP, VP]),
     "raptr_matrix_csc_info": (C.c_int, [VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP)]),
     "raptr_csr_transpose": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP]),
+    "raptr_mlem_noalloc": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, I32, VP]),
     "raptr_reco_host": (C.c_int, [C.POINTER(raptr_geom), C.c_int, VP, I32, C.c_uint32, I32, VP, VP, VP,
                                   C.POINTER(raptr_reco_stats)]),
 }

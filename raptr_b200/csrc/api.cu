@@ -787,6 +787,15 @@ raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_r
   return RAPTR_OK;
 }
 
+raptr_status raptr_mlem_noalloc(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                                const float* d_val, const float* d_y, const float* d_s, float* d_x, int32_t n_iter,
+                                void* stream) {
+  std::string err;
+  raptr_status st = mlem_noalloc(m, n, d_row_ptr, d_col, d_val, d_y, d_s, d_x, n_iter, as_stream(stream), &err);
+  if (st != RAPTR_OK) return fail(st, err);
+  return RAPTR_OK;
+}
+
 // ---- end-to-end -----------------------------------------------------------------------
 
 raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_y, int32_t nrays, uint32_t seed,

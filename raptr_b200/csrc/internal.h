@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -113,5 +114,10 @@ cudaError_t launch_mlem_back(int64_t n, const int64_t* cp, const int32_t* trow, 
                              const float* x, const float* sens, float* out, double* d_acc, bool update,
                              cudaStream_t s);
 cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s);
+
+// MLEM with its workspace in a fixed device array (mlem_noalloc.cu).
+raptr_status mlem_noalloc(int64_t m, int64_t n, const int64_t* rp, const int32_t* col, const float* val,
+                          const float* y, const float* s, float* x, int32_t n_iter, cudaStream_t st,
+                          std::string* err);
 
 }  // namespace raptr
