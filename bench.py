@@ -284,27 +284,28 @@ def run_job(R, torch, ctx, w, lst, y_dev, dist=None):
     ev[1].record()
     A.transpose()
     ev[2].record()
-    s64, s = R.sensitivity(A)
-    if dist is not None:
-        dist.all_reduce(s64)
-        s = (s64 / s64.sum()).float()
+    if dist is None:
+        s64, s = R.sensitivity(A)
+    else:
+        from raptr_b200.distributed import GpuShardOps, ShardedMLEM
+
+        sharded = ShardedMLEM(GpuShardOps(A), dist)
+        s = sharded.sensitivity()
     ev[3].record()
     x = torch.full((g.n_voxels,), np.float32(1.0 / g.n_voxels), device="cuda")
     if dist is None:
         kt = ctx.mlem(A, y_dev, s, x, w["niter"], use_graph=False, kernel_times=True)
     else:
-        e = torch.empty(A.m, device="cuda")
-        c = torch.empty(g.n_voxels, device="cuda")
-        acc = torch.zeros(1, dtype=torch.float64, device="cuda")
+        ops = sharded.ops
         kev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(w["niter"])]
-        for it in range(w["niter"]):
+        for it in range(w["niter"]):  # ShardedMLEM.iterate, with events around the two passes
             kev[it][0].record()
-            R.mlem_forward(A, y_dev, x, e)
+            e = ops.forward(y_dev, x)
             kev[it][1].record()
-            R.mlem_back(A, e, c)
+            c = ops.back(e)
             kev[it][2].record()
             dist.all_reduce(c)
-            R.mlem_update(x, c, s, acc)
+            ops.update(x, c, s)
         torch.cuda.synchronize()
         kt = np.array([[k[0].elapsed_time(k[1]), k[1].elapsed_time(k[2])] for k in kev])
     ev[4].record()

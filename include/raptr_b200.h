@@ -163,6 +163,13 @@ raptr_status raptr_coo2csr(const int32_t* d_rows, int64_t nnz, int64_t m, int64_
 raptr_status raptr_csr2ecsr(int64_t* d_ecsr, const int32_t* d_yrow, int64_t nnzr, const int64_t* d_csr, int64_t m,
                             void* stream);
 
+/* Row pointers between the reference's int32 CSR (src/cusparseWrapper.hpp:53-60,
+ * src/csrmv.hpp:61-66) and the int64 ones used here.  Narrowing checks the
+ * last (largest) pointer and returns RAPTR_ERR_INVALID when it exceeds
+ * INT32_MAX; it synchronises the stream for that check. */
+raptr_status raptr_row_ptr_narrow(const int64_t* d_in, int64_t n, int32_t* d_out, void* stream);
+raptr_status raptr_row_ptr_widen(const int32_t* d_in, int64_t n, int64_t* d_out, void* stream);
+
 /* ---- SpMV ---------------------------------------------------------------- */
 
 #define RAPTR_OP_N 0 /* y = alpha*A*x   + beta*y  (forward projection) */

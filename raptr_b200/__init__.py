@@ -120,6 +120,8 @@ _SIGNATURES = {
     "raptr_matrix_csc_info": (C.c_int, [VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP)]),
     "raptr_csr_transpose": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_mlem_noalloc": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, I32, VP]),
+    "raptr_row_ptr_narrow": (C.c_int, [VP, I64, VP, VP]),
+    "raptr_row_ptr_widen": (C.c_int, [VP, I64, VP, VP]),
     "raptr_reco_host": (C.c_int, [C.POINTER(raptr_geom), C.c_int, VP, I32, C.c_uint32, I32, VP, VP, VP,
                                   C.POINTER(raptr_reco_stats)]),
 }

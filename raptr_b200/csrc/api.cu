@@ -7,6 +7,7 @@
 // src/MeasurementSetupTrafo2CartCoord.hpp:110-111; it is compiled with
 // -ffp-contract=off so the expression is evaluated as written.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -580,6 +581,25 @@ raptr_status raptr_csr2ecsr(int64_t* d_ecsr, const int32_t* d_yrow, int64_t nnzr
                             void* stream) {
   if (nnzr < 0 || m < 0 || !d_ecsr || !d_csr || (nnzr > 0 && !d_yrow)) return fail(RAPTR_ERR_INVALID, "bad argument");
   RCU(launch_csr2ecsr(d_ecsr, d_yrow, nnzr, d_csr, m, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_row_ptr_narrow(const int64_t* d_in, int64_t n, int32_t* d_out, void* stream) {
+  if (n < 0 || (n > 0 && (!d_in || !d_out))) return fail(RAPTR_ERR_INVALID, "bad argument");
+  if (n == 0) return RAPTR_OK;
+  cudaStream_t s = as_stream(stream);
+  int64_t last = 0;
+  RCU(cudaMemcpyAsync(&last, d_in + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  RCU(cudaStreamSynchronize(s));
+  if (last > int64_t(INT32_MAX) || last < 0)
+    return fail(RAPTR_ERR_INVALID, "row pointer " + std::to_string(last) + " does not fit in int32");
+  RCU(launch_narrow_i64(d_in, n, d_out, s));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_row_ptr_widen(const int32_t* d_in, int64_t n, int64_t* d_out, void* stream) {
+  if (n < 0 || (n > 0 && (!d_in || !d_out))) return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_widen_i32(d_in, n, d_out, as_stream(stream)));
   return RAPTR_OK;
 }
 

@@ -114,6 +114,8 @@ cudaError_t launch_mlem_back(int64_t n, const int64_t* cp, const int32_t* trow, 
                              const float* x, const float* sens, float* out, double* d_acc, bool update,
                              cudaStream_t s);
 cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s);
+cudaError_t launch_narrow_i64(const int64_t* in, int64_t n, int32_t* out, cudaStream_t s);
+cudaError_t launch_widen_i32(const int32_t* in, int64_t n, int64_t* out, cudaStream_t s);
 
 // MLEM with its workspace in a fixed device array (mlem_noalloc.cu).
 raptr_status mlem_noalloc(int64_t m, int64_t n, const int64_t* rp, const int32_t* col, const float* val,

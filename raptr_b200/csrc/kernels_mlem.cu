@@ -60,22 +60,29 @@ __device__ __forceinline__ float row_dot(const int32_t* __restrict__ col, const 
   const int4* c4 = reinterpret_cast<const int4*>(col + a);
   const float4* v4 = reinterpret_cast<const float4*>(val + a);
   int64_t q = lane;
-  for (; q + 32 < nq; q += 64) {
-    int4 c0 = __ldg(c4 + q);
-    float4 w0 = __ldg(v4 + q);
-    int4 c1 = __ldg(c4 + q + 32);
-    float4 w1 = __ldg(v4 + q + 32);
-    acc += w0.x * __ldg(x + c0.x) + w0.y * __ldg(x + c0.y) + w0.z * __ldg(x + c0.z) + w0.w * __ldg(x + c0.w);
-    acc += w1.x * __ldg(x + c1.x) + w1.y * __ldg(x + c1.y) + w1.z * __ldg(x + c1.z) + w1.w * __ldg(x + c1.w);
+  // Four quads (16 entries) per lane per step: 8 independent 16-byte loads,
+  // then 16 independent gathers, kept in flight together.
+  float acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+  for (; q + 96 < nq; q += 128) {
+    const int4 c0 = __ldg(c4 + q), c1 = __ldg(c4 + q + 32), c2 = __ldg(c4 + q + 64), c3 = __ldg(c4 + q + 96);
+    const float4 w0 = __ldg(v4 + q), w1 = __ldg(v4 + q + 32), w2 = __ldg(v4 + q + 64), w3 = __ldg(v4 + q + 96);
+    const float g00 = __ldg(x + c0.x), g01 = __ldg(x + c0.y), g02 = __ldg(x + c0.z), g03 = __ldg(x + c0.w);
+    const float g10 = __ldg(x + c1.x), g11 = __ldg(x + c1.y), g12 = __ldg(x + c1.z), g13 = __ldg(x + c1.w);
+    const float g20 = __ldg(x + c2.x), g21 = __ldg(x + c2.y), g22 = __ldg(x + c2.z), g23 = __ldg(x + c2.w);
+    const float g30 = __ldg(x + c3.x), g31 = __ldg(x + c3.y), g32 = __ldg(x + c3.z), g33 = __ldg(x + c3.w);
+    acc += w0.x * g00 + w0.y * g01 + w0.z * g02 + w0.w * g03;
+    acc1 += w1.x * g10 + w1.y * g11 + w1.z * g12 + w1.w * g13;
+    acc2 += w2.x * g20 + w2.y * g21 + w2.z * g22 + w2.w * g23;
+    acc3 += w3.x * g30 + w3.y * g31 + w3.z * g32 + w3.w * g33;
   }
-  if (q < nq) {
-    int4 c0 = __ldg(c4 + q);
-    float4 w0 = __ldg(v4 + q);
+  for (; q < nq; q += 32) {
+    const int4 c0 = __ldg(c4 + q);
+    const float4 w0 = __ldg(v4 + q);
     acc += w0.x * __ldg(x + c0.x) + w0.y * __ldg(x + c0.y) + w0.z * __ldg(x + c0.z) + w0.w * __ldg(x + c0.w);
   }
   const int64_t t = a + (nq << 2) + lane;
   if (t < e) acc += __ldg(val + t) * __ldg(x + __ldg(col + t));
-  return warp_sum(acc);
+  return warp_sum((acc + acc1) + (acc2 + acc3));
 }
 
 // y[col] += f * val over CSR row [b, e), by one warp.  Streaming loads:

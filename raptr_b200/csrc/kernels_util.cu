@@ -123,6 +123,16 @@ __global__ void iota_kernel(int32_t* __restrict__ p, int64_t n) {
     p[i] = int32_t(i);
 }
 
+__global__ void narrow_kernel(const int64_t* __restrict__ in, int64_t n, int32_t* __restrict__ out) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = int32_t(in[i]);
+}
+
+__global__ void widen32_kernel(const int32_t* __restrict__ in, int64_t n, int64_t* __restrict__ out) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = in[i];
+}
+
 unsigned grid_for(int64_t n, int threads) {
   int64_t b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -135,6 +145,22 @@ unsigned grid_for(int64_t n, int threads) {
 cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s) {
   if (n > 0) {
     iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, n);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_narrow_i64(const int64_t* in, int64_t n, int32_t* out, cudaStream_t s) {
+  if (n > 0) {
+    narrow_kernel<<<grid_for(n, 256), 256, 0, s>>>(in, n, out);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_widen_i32(const int32_t* in, int64_t n, int64_t* out, cudaStream_t s) {
+  if (n > 0) {
+    widen32_kernel<<<grid_for(n, 256), 256, 0, s>>>(in, n, out);
     note_launches(1);
   }
   return cudaGetLastError();
