@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define RAPTR_ABI_VERSION 1
+#define RAPTR_ABI_VERSION 2
 
 typedef enum raptr_status {
   RAPTR_OK = 0,
@@ -142,19 +142,44 @@ raptr_status raptr_matrix_destroy(raptr_matrix* A);
 
 /* Transpose (CSC) of the library matrix, built once and kept resident beside
  * the CSR (same values, grouped by voxel): back projection then gathers by
- * columns instead of scattering with atomics.  Synchronises the stream. */
+ * columns instead of scattering with atomics.  Synchronises the stream.
+ * The columns list the rows in the matrix's back-projection order: channels
+ * sorted by (angle, z0+z1, y0+y1, z0-z1, y0-y1), so that the channels
+ * crossing one voxel are few dense runs of that order.  The CSC's row
+ * index is then the position k in that order (row = order[k]; see
+ * raptr_matrix_row_order) and a vector it is applied to is laid out the
+ * same way (raptr_mlem_forward_ordered writes it so).  A matrix whose list
+ * repeats a channel keeps the natural order (order and rank null, the row
+ * index is the row).  Entries within a column are ascending in k, so
+ * results do not depend on scheduling. */
 raptr_status raptr_matrix_transpose(raptr_matrix* A, void* stream);
 /* Pointers of the transpose (null until raptr_matrix_transpose). */
 raptr_status raptr_matrix_csc_info(const raptr_matrix* A, int64_t** d_col_ptr, int32_t** d_row_idx, float** d_tval);
+/* Back-projection order of the rows after raptr_matrix_transpose:
+ * d_order[k] = row at position k, d_rank[row] = its position (m int32 each);
+ * both null for the natural order. */
+raptr_status raptr_matrix_row_order(const raptr_matrix* A, int32_t** d_order, int32_t** d_rank);
 
 /* ---- sparse formats --------------------------------------------------------- */
 
 /* CSC of an m x n CSR matrix into caller buffers: d_col_ptr (n+1 int64),
- * d_row_idx and d_tval (nnz each).  Within a column the row order is not
- * specified. */
+ * d_row_idx and d_tval (nnz each).  Within a column the rows are ascending
+ * (the result does not depend on scheduling).  Replaces the transposed
+ * cusparse csrmv of src/csrmv.hpp:61-66 as a stored CSC.  Synchronises the
+ * stream; column indices outside [0, n) give RAPTR_ERR_INVALID. */
 raptr_status raptr_csr_transpose(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
                                  const float* d_val, int64_t* d_col_ptr, int32_t* d_row_idx, float* d_tval,
                                  void* stream);
+/* The same with the rows taken in a caller order: d_order (m int32) is a
+ * permutation of [0, m), row d_order[k] is the k-th; within each column the
+ * entries are ascending in k and d_pos_idx holds k instead of the row.  No
+ * counterpart in the reference.  Back projection through this CSC reads a
+ * vector laid out in the same order (v_k = e[d_order[k]]); an order that
+ * puts rows crossing the same voxels next to each other makes those reads
+ * dense. */
+raptr_status raptr_csr_transpose_ordered(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                                         const float* d_val, const int32_t* d_order, int64_t* d_col_ptr,
+                                         int32_t* d_pos_idx, float* d_tval, void* stream);
 
 /* Row pointers (m+1 int64) from sorted COO row indices (nnz int32). */
 raptr_status raptr_coo2csr(const int32_t* d_rows, int64_t nnz, int64_t m, int64_t* d_row_ptr, void* stream);
@@ -202,6 +227,9 @@ typedef struct raptr_mlem_opts {
   float* h_kernel_ms;  /* optional: 2*n_iter device times (ms) of the two passes of
                           each iteration, from CUDA events on the stream; when
                           set the loop is launched without a graph             */
+  const int32_t* d_row_rank; /* optional, with the transpose: the CSC's row
+                          index is the position in an order, d_row_rank[row]
+                          the row's position (raptr_matrix_row_order)         */
 } raptr_mlem_opts;
 
 /* n_iter MLEM iterations in the order of src/tests/reco.cu:230-303:
@@ -236,6 +264,11 @@ raptr_status raptr_mlem_forward(int64_t m, const int64_t* d_row_ptr, const int32
                                 const float* d_y, const float* d_x, float* d_e, double* d_ll, void* stream);
 raptr_status raptr_mlem_back(int64_t n, const int64_t* d_col_ptr, const int32_t* d_row_idx, const float* d_tval,
                              const float* d_e, float* d_c, void* stream);
+/* raptr_mlem_forward storing e_i at d_e[d_row_rank[i]], the layout that
+ * raptr_mlem_back reads through a transpose in that order. */
+raptr_status raptr_mlem_forward_ordered(int64_t m, const int64_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                                        const float* d_y, const float* d_x, const int32_t* d_row_rank, float* d_e,
+                                        double* d_ll, void* stream);
 
 /* MLEM iterations that allocate no device memory.  No counterpart in the
  * reference (which allocates its buffers itself).  For callers that cannot

@@ -54,7 +54,8 @@ class raptr_geom(C.Structure):
 
 
 class raptr_mlem_opts(C.Structure):
-    _fields_ = [("use_graph", C.c_int32), ("h_loglik", C.POINTER(C.c_double)), ("h_kernel_ms", C.POINTER(C.c_float))]
+    _fields_ = [("use_graph", C.c_int32), ("h_loglik", C.POINTER(C.c_double)), ("h_kernel_ms", C.POINTER(C.c_float)),
+                ("d_row_rank", C.c_void_p)]
 
 
 class raptr_reco_stats(C.Structure):
@@ -115,10 +116,13 @@ _SIGNATURES = {
     "raptr_mlem": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32, C.POINTER(raptr_mlem_opts),
                              VP]),
     "raptr_mlem_forward": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, VP, VP]),
+    "raptr_mlem_forward_ordered": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_mlem_back": (C.c_int, [I64, VP, VP, VP, VP, VP, VP]),
     "raptr_matrix_transpose": (C.c_int, [VP, VP]),
     "raptr_matrix_csc_info": (C.c_int, [VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP)]),
+    "raptr_matrix_row_order": (C.c_int, [VP, C.POINTER(VP), C.POINTER(VP)]),
     "raptr_csr_transpose": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP]),
+    "raptr_csr_transpose_ordered": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_mlem_noalloc": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, I32, VP]),
     "raptr_row_ptr_narrow": (C.c_int, [VP, I64, VP, VP]),
     "raptr_row_ptr_widen": (C.c_int, [VP, I64, VP, VP]),
@@ -219,6 +223,10 @@ class Matrix:
         return self.col_ptr is not None
 
     col_ptr = None
+    # back-projection order of the rows (row_idx of the transpose holds
+    # positions k, row = row_order[k]); None for the natural order
+    row_order = None
+    row_rank = None
     row_idx = None
     tval = None
 
@@ -237,6 +245,11 @@ class Matrix:
         else:
             self.row_idx = torch.zeros(0, dtype=torch.int32, device=dev)
             self.tval = torch.zeros(0, dtype=torch.float32, device=dev)
+        order, rank = VP(), VP()
+        _check(lib().raptr_matrix_row_order(self._h, C.byref(order), C.byref(rank)))
+        if order.value and self.m > 0:
+            self.row_order = torch.as_tensor(_DeviceArray(order.value, (self.m,), "<i4", own), device=dev)
+            self.row_rank = torch.as_tensor(_DeviceArray(rank.value, (self.m,), "<i4", own), device=dev)
         return self
 
     def to_numpy(self):
@@ -338,7 +351,8 @@ class Context:
         ll = (C.c_double * max(niter, 1))() if loglik else None
         kt = (C.c_float * max(2 * niter, 1))() if kernel_times else None
         opts = raptr_mlem_opts(1 if use_graph else 0, C.cast(ll, C.POINTER(C.c_double)) if loglik else None,
-                               C.cast(kt, C.POINTER(C.c_float)) if kernel_times else None)
+                               C.cast(kt, C.POINTER(C.c_float)) if kernel_times else None,
+                               _ptr(A.row_rank) if A.has_transpose else None)
         _check(lib().raptr_mlem(self._h, A.m, A.n, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(A.col_ptr),
                                 _ptr(A.row_idx), _ptr(A.tval), _ptr(y), _ptr(s), _ptr(x), niter, C.byref(opts),
                                 _stream(stream)))
@@ -378,6 +392,13 @@ def mlem_project(A: Matrix, y, x, c, ll=None, stream=None):
 
 
 def mlem_forward(A: Matrix, y, x, e, ll=None, stream=None):
+    """e = y / (A x) (0 where y == 0), laid out as mlem_back(A, ...) reads it:
+    in A's back-projection order when its transpose has one (e[row_rank[i]]
+    for row i), else by row."""
+    if A.row_rank is not None:
+        _check(lib().raptr_mlem_forward_ordered(A.m, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(y), _ptr(x),
+                                                _ptr(A.row_rank), _ptr(e), _ptr(ll), _stream(stream)))
+        return
     _check(lib().raptr_mlem_forward(A.m, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(y), _ptr(x), _ptr(e),
                                     _ptr(ll), _stream(stream)))
 
@@ -395,6 +416,19 @@ def csr_transpose(m: int, n: int, row_ptr, col, val, stream=None):
     tv = torch.empty(max(col.numel(), 1), dtype=torch.float32, device=row_ptr.device)
     _check(lib().raptr_csr_transpose(m, n, _ptr(row_ptr), _ptr(col), _ptr(val), _ptr(cp), _ptr(ri), _ptr(tv),
                                      _stream(stream)))
+    return cp, ri[:col.numel()], tv[:col.numel()]
+
+
+def csr_transpose_ordered(m: int, n: int, row_ptr, col, val, order, stream=None):
+    """CSC with the rows taken in `order` (a permutation of range(m)); the
+    returned index array holds positions k in that order, ascending within
+    each column."""
+    torch = _torch()
+    cp = torch.empty(n + 1, dtype=torch.int64, device=row_ptr.device)
+    ri = torch.empty(max(col.numel(), 1), dtype=torch.int32, device=row_ptr.device)
+    tv = torch.empty(max(col.numel(), 1), dtype=torch.float32, device=row_ptr.device)
+    _check(lib().raptr_csr_transpose_ordered(m, n, _ptr(row_ptr), _ptr(col), _ptr(val), _ptr(order), _ptr(cp),
+                                             _ptr(ri), _ptr(tv), _stream(stream)))
     return cp, ri[:col.numel()], tv[:col.numel()]
 
 

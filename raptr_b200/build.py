@@ -25,6 +25,7 @@ UNITS = {
     "kernels_sm.cu": ["-fmad=false"],
     "kernels_util.cu": [],
     "kernels_mlem.cu": [],
+    "kernels_transpose.cu": [],
     "mlem_noalloc.cu": [],
 }
 

@@ -138,6 +138,13 @@ struct raptr_matrix {
   int64_t* cp = nullptr;
   int32_t* trow = nullptr;
   float* tval = nullptr;
+  // channel of each row (matrices built by the library) and the geometry
+  // they belong to: the transpose is then built in the back-projection order
+  // of the channels, trow holding positions in that order
+  int32_t* cnl = nullptr;
+  DGeom geom{};
+  int32_t* rank = nullptr;   // row -> position
+  int32_t* order = nullptr;  // position -> row
 };
 
 namespace {
@@ -475,6 +482,17 @@ raptr_status raptr_sm_build_alloc(raptr_ctx* ctx, const int32_t* d_cnl_ids, int6
     return st;
   }
   A->nnz = nnz;
+  A->geom = ctx->dg;
+  if (n_list > 0) {
+    cudaError_t ec = cudaMalloc(&A->cnl, size_t(n_list) * sizeof(int32_t));
+    if (ec == cudaSuccess)
+      ec = cudaMemcpyAsync(A->cnl, d_cnl_ids, size_t(n_list) * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                           as_stream(stream));
+    if (ec != cudaSuccess) {
+      raptr_matrix_destroy(A);
+      return cuda_fail(ec, "cudaMalloc(channel list)");
+    }
+  }
   *out_m = A;
   return RAPTR_OK;
 }
@@ -500,65 +518,190 @@ raptr_status raptr_matrix_destroy(raptr_matrix* A) {
   cudaFree(A->cp);
   cudaFree(A->trow);
   cudaFree(A->tval);
+  cudaFree(A->cnl);
+  cudaFree(A->rank);
+  cudaFree(A->order);
   delete A;
   return RAPTR_OK;
 }
 
-raptr_status raptr_csr_transpose(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
-                                 const float* d_val, int64_t* d_col_ptr, int32_t* d_row_idx, float* d_tval,
-                                 void* stream) {
-  if (m < 0 || n <= 0 || !d_row_ptr || !d_col_ptr) return fail(RAPTR_ERR_INVALID, "bad argument");
-  cudaStream_t s = as_stream(stream);
+namespace {
+
+raptr_status transpose_impl(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                            const int32_t* d_order, int64_t* d_col_ptr, int32_t* d_row_idx, float* d_tval,
+                            cudaStream_t s) {
+  if (m < 0 || n <= 0 || m > INT32_MAX || n > INT32_MAX || !d_row_ptr || !d_col_ptr)
+    return fail(RAPTR_ERR_INVALID, "bad argument");
   int64_t nnz = 0;
   RCU(cudaMemcpyAsync(&nnz, d_row_ptr + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   RCU(cudaStreamSynchronize(s));
   if (nnz > 0 && (!d_col || !d_val || !d_row_idx || !d_tval)) return fail(RAPTR_ERR_INVALID, "null buffer");
-  int32_t* cnt = nullptr;
-  int64_t *wide = nullptr, *tmp = nullptr;
-  RCU(cudaMallocAsync(&cnt, size_t(n) * sizeof(int32_t), s));
-  cudaError_t e = cudaMallocAsync(&wide, size_t(n) * sizeof(int64_t), s);
+  // radix sort by column when it applies and its staging (12 bytes per
+  // entry) fits; else the blocked transpose (4 bytes per column and block)
+  RadixPlan plan;
+  if (nnz > 0 && transpose_radix_plan(m, n, nnz, &plan)) {
+    const int64_t nh = radix_hist_elems(plan);
+    int64_t *hist = nullptr, *off = nullptr, *tmp = nullptr, *cc64 = nullptr;
+    int32_t *cc = nullptr, *bad = nullptr, *st_key = nullptr, *st_k = nullptr;
+    float* st_v = nullptr;
+    // plain allocations: the stream-ordered pool grows slowly at these
+    // sizes (the staging is tens of GB at full size)
+    cudaError_t e = cudaMalloc(&hist, size_t(nh) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&off, size_t(nh + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, size_t(scan_temp_elems(std::max(nh, n))) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&cc, size_t(n) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&cc64, size_t(n) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&bad, sizeof(int32_t));
+    bool staged = true;
+    if (e == cudaSuccess && plan.passes > 1) {
+      if (cudaMalloc(&st_key, size_t(nnz) * sizeof(int32_t)) != cudaSuccess ||
+          cudaMalloc(&st_k, size_t(nnz) * sizeof(int32_t)) != cudaSuccess ||
+          cudaMalloc(&st_v, size_t(nnz) * sizeof(float)) != cudaSuccess) {
+        (void)cudaGetLastError();  // does not fit: the blocked transpose needs less
+        staged = false;
+      }
+    }
+    int32_t h_bad = 0;
+    if (e == cudaSuccess && staged) {
+      e = cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
+      if (e == cudaSuccess)
+        e = launch_transpose_radix(plan, m, n, nnz, d_row_ptr, d_col, d_val, d_order, hist, off, tmp, cc, cc64,
+                                   st_key, st_k, st_v, bad, d_col_ptr, d_row_idx, d_tval, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(hist);
+    cudaFree(off);
+    cudaFree(tmp);
+    cudaFree(cc);
+    cudaFree(cc64);
+    cudaFree(bad);
+    cudaFree(st_key);
+    cudaFree(st_k);
+    cudaFree(st_v);
+    if (e != cudaSuccess) return cuda_fail(e, "raptr_csr_transpose");
+    if (h_bad) return fail(RAPTR_ERR_INVALID, "column index or row order entry out of range");
+    if (staged) return RAPTR_OK;
+  }
+  const int B = transpose_blocks(m, n);
+  int32_t *cnt = nullptr, *bad = nullptr;
+  int64_t *colcount = nullptr, *tmp = nullptr;
+  cudaError_t e = cudaMallocAsync(&cnt, size_t(B) * size_t(n) * sizeof(int32_t), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&colcount, size_t(n) * sizeof(int64_t), s);
   if (e == cudaSuccess) e = cudaMallocAsync(&tmp, size_t(scan_temp_elems(n)) * sizeof(int64_t), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, size_t(n) * sizeof(int32_t), s);
-  if (e == cudaSuccess) e = launch_column_counts(nnz, d_col, cnt, s);
-  if (e == cudaSuccess) e = launch_widen(n, cnt, wide, s);
-  if (e == cudaSuccess) e = launch_scan_i64(wide, n, d_col_ptr, tmp, s);
-  // cursors start at the column pointers
-  if (e == cudaSuccess) e = cudaMemcpyAsync(wide, d_col_ptr, size_t(n) * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
-  if (e == cudaSuccess) e = launch_transpose_fill(m, d_row_ptr, d_col, d_val, wide, d_row_idx, d_tval, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&bad, sizeof(int32_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
+  if (e == cudaSuccess)
+    e = launch_transpose_blocked(m, n, B, d_row_ptr, d_col, d_val, d_order, d_order != nullptr, cnt, colcount, tmp,
+                                 bad, d_col_ptr, d_row_idx, d_tval, s);
+  int32_t h_bad = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   if (cnt) cudaFreeAsync(cnt, s);
-  if (wide) cudaFreeAsync(wide, s);
+  if (colcount) cudaFreeAsync(colcount, s);
   if (tmp) cudaFreeAsync(tmp, s);
+  if (bad) cudaFreeAsync(bad, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "raptr_csr_transpose");
+  if (h_bad) return fail(RAPTR_ERR_INVALID, "column index or row order entry out of range");
   return RAPTR_OK;
 }
+
+}  // namespace
+
+raptr_status raptr_csr_transpose(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                                 const float* d_val, int64_t* d_col_ptr, int32_t* d_row_idx, float* d_tval,
+                                 void* stream) {
+  return transpose_impl(m, n, d_row_ptr, d_col, d_val, nullptr, d_col_ptr, d_row_idx, d_tval, as_stream(stream));
+}
+
+raptr_status raptr_csr_transpose_ordered(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                                         const float* d_val, const int32_t* d_order, int64_t* d_col_ptr,
+                                         int32_t* d_pos_idx, float* d_tval, void* stream) {
+  if (m > 0 && !d_order) return fail(RAPTR_ERR_INVALID, "order is null");
+  return transpose_impl(m, n, d_row_ptr, d_col, d_val, d_order, d_col_ptr, d_pos_idx, d_tval, as_stream(stream));
+}
+
+namespace {
+
+// Back-projection order of the rows of a library-built matrix (its
+// channels): fills A->rank / A->order and sets *have.  Leaves the natural
+// order (*have false) when the rows repeat a channel or the key space is
+// too large to mark.
+cudaError_t matrix_row_order(raptr_matrix* A, cudaStream_t s, bool* have) {
+  *have = false;
+  if (!A->cnl || A->m <= 0) return cudaSuccess;
+  const int64_t K = channel_order_keys(A->geom);
+  if (K <= 0 || K > (int64_t(1) << 28)) return cudaSuccess;
+  unsigned long long* mark = nullptr;
+  int64_t *prefix = nullptr, *tmp = nullptr;
+  int32_t* bad = nullptr;
+  // plain allocations: the stream-ordered pool grows slowly at this size
+  cudaError_t e = cudaMalloc(&mark, size_t(K) * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&prefix, size_t(K + 1) * sizeof(int64_t));
+  if (e == cudaSuccess) e = cudaMalloc(&tmp, size_t(scan_temp_elems(K)) * sizeof(int64_t));
+  if (e == cudaSuccess) e = cudaMalloc(&bad, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
+  if (e == cudaSuccess) e = launch_channel_order_mark(A->geom, A->m, A->cnl, mark, bad, s);
+  if (e == cudaSuccess) e = launch_scan_i64(reinterpret_cast<const int64_t*>(mark), K, prefix, tmp, s);
+  int32_t h_bad = 1;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess && !h_bad) {
+    e = cudaMalloc(&A->rank, size_t(A->m) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&A->order, size_t(A->m) * sizeof(int32_t));
+    if (e == cudaSuccess) e = launch_channel_order_rank(A->geom, A->m, A->cnl, prefix, A->rank, A->order, s);
+    if (e == cudaSuccess) {
+      *have = true;
+    } else {
+      cudaFree(A->rank);
+      cudaFree(A->order);
+      A->rank = A->order = nullptr;
+    }
+  }
+  cudaFree(mark);
+  cudaFree(prefix);
+  cudaFree(tmp);
+  cudaFree(bad);
+  return e;
+}
+
+}  // namespace
 
 raptr_status raptr_matrix_transpose(raptr_matrix* A, void* stream) {
   if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
   if (A->cp) return RAPTR_OK;
   DeviceScope ds(A->device);
-  RCU(cudaMalloc(&A->cp, size_t(A->n + 1) * sizeof(int64_t)));
-  cudaError_t e = cudaMalloc(&A->trow, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(int32_t));
+  cudaStream_t s = as_stream(stream);
+  bool ordered = false;
+  RCU(matrix_row_order(A, s, &ordered));
+  cudaError_t e = cudaMalloc(&A->cp, size_t(A->n + 1) * sizeof(int64_t));
+  if (e == cudaSuccess) e = cudaMalloc(&A->trow, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMalloc(&A->tval, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(float));
-  if (e != cudaSuccess) {
-    cudaFree(A->cp);
-    cudaFree(A->trow);
-    cudaFree(A->tval);
-    A->cp = nullptr;
-    A->trow = nullptr;
-    A->tval = nullptr;
-    return cuda_fail(e, "cudaMalloc(transpose)");
-  }
-  raptr_status st = raptr_csr_transpose(A->m, A->n, A->rp, A->col, A->val, A->cp, A->trow, A->tval, stream);
+  raptr_status st = RAPTR_OK;
+  if (e != cudaSuccess)
+    st = cuda_fail(e, "cudaMalloc(transpose)");
+  else
+    st = transpose_impl(A->m, A->n, A->rp, A->col, A->val, ordered ? A->order : nullptr, A->cp, A->trow, A->tval, s);
   if (st != RAPTR_OK) {
     cudaFree(A->cp);
     cudaFree(A->trow);
     cudaFree(A->tval);
+    cudaFree(A->rank);
+    cudaFree(A->order);
     A->cp = nullptr;
     A->trow = nullptr;
     A->tval = nullptr;
+    A->rank = A->order = nullptr;
   }
   return st;
+}
+
+raptr_status raptr_matrix_row_order(const raptr_matrix* A, int32_t** d_order, int32_t** d_rank) {
+  if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
+  if (d_order) *d_order = A->order;
+  if (d_rank) *d_rank = A->rank;
+  return RAPTR_OK;
 }
 
 raptr_status raptr_matrix_csc_info(const raptr_matrix* A, int64_t** d_col_ptr, int32_t** d_row_idx, float** d_tval) {
@@ -685,7 +828,16 @@ raptr_status raptr_mlem_update(int64_t n, float* d_x, float* d_c, const float* d
 raptr_status raptr_mlem_forward(int64_t m, const int64_t* d_row_ptr, const int32_t* d_col, const float* d_val,
                                 const float* d_y, const float* d_x, float* d_e, double* d_ll, void* stream) {
   if (m < 0 || !d_row_ptr || !d_y || !d_x || !d_e) return fail(RAPTR_ERR_INVALID, "bad argument");
-  RCU(launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, d_e, d_ll, as_stream(stream)));
+  RCU(launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, nullptr, d_e, d_ll, as_stream(stream)));
+  return RAPTR_OK;
+}
+
+raptr_status raptr_mlem_forward_ordered(int64_t m, const int64_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                                        const float* d_y, const float* d_x, const int32_t* d_row_rank, float* d_e,
+                                        double* d_ll, void* stream) {
+  if (m < 0 || !d_row_ptr || !d_y || !d_x || !d_e || (m > 0 && !d_row_rank))
+    return fail(RAPTR_ERR_INVALID, "bad argument");
+  RCU(launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, d_row_rank, d_e, d_ll, as_stream(stream)));
   return RAPTR_OK;
 }
 
@@ -710,6 +862,7 @@ raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_r
   const bool want_times = opts && opts->h_kernel_ms;
   const bool use_graph = opts && opts->use_graph && !want_times;
   const bool csc = d_col_ptr != nullptr;
+  const int32_t* rank = opts ? opts->d_row_rank : nullptr;
   std::vector<cudaEvent_t> evs;
   if (want_times) {
     evs.resize(size_t(3 * n_iter));
@@ -731,7 +884,8 @@ raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_r
       cudaError_t err = cudaMemsetAsync(acc, 0, sizeof(double), q);
       if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it)], q);
       if (csc) {
-        if (err == cudaSuccess) err = launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, e, lli, q);
+        if (err == cudaSuccess)
+          err = launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, rank, e, lli, q);
         if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 1)], q);
         if (err == cudaSuccess) err = launch_mlem_back(n, d_col_ptr, d_row_idx, d_tval, e, d_x, d_s, c, acc, true, q);
         if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 2)], q);
@@ -906,7 +1060,7 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
     h2d += N * int64_t(sizeof(float));
   }
   RSTEP(cudaEventRecord(ev[3], s));
-  raptr_mlem_opts o{1, nullptr, nullptr};
+  raptr_mlem_opts o{1, nullptr, nullptr, A->rank};
   st = raptr_mlem(ctx, A->m, N, A->rp, A->col, A->val, A->cp, A->trow, A->tval, d_y, d_s, d_x, n_iter, &o, s);
   if (st != RAPTR_OK) {
     std::string msg = g_last_error;

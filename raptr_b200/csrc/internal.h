@@ -102,13 +102,48 @@ cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s);
 
 // Transpose (CSC) of a CSR matrix: column counts (int32 atomics), widening to
 // int64, and the fill through per-column cursors (initialised to col_ptr).
-cudaError_t launch_column_counts(int64_t nnz, const int32_t* col, int32_t* cnt, cudaStream_t s);
-cudaError_t launch_widen(int64_t n, const int32_t* a, int64_t* b, cudaStream_t s);
-cudaError_t launch_transpose_fill(int64_t m, const int64_t* rp, const int32_t* col, const float* val,
-                                  int64_t* cursor, int32_t* trow, float* tval, cudaStream_t s);
+// Back-projection order of a list of channels (kernels_util.cu): key per
+// channel in [0, channel_order_keys(g)); mark counts keys (bad |= 1 on a
+// repeated key or a channel out of range); with prefix = exclusive scan of
+// mark, rank[r] = prefix[key(cnl[r])] and order[rank[r]] = r.
+int64_t channel_order_keys(const DGeom& g);
+cudaError_t launch_channel_order_mark(const DGeom& g, int64_t m, const int32_t* cnl, unsigned long long* mark,
+                                      int32_t* bad, cudaStream_t s);
+cudaError_t launch_channel_order_rank(const DGeom& g, int64_t m, const int32_t* cnl, const int64_t* prefix,
+                                      int32_t* rank, int32_t* order, cudaStream_t s);
+
+// Radix-sort CSR -> CSC (kernels_transpose.cu): the same result as the
+// blocked transpose below, for n <= 2^20.  Buffers: hist and off
+// radix_hist_elems(plan) (+1 for off) int64, scan_tmp
+// scan_temp_elems(max(radix_hist_elems, n)) int64, colcnt n int32, colcnt64
+// n int64, staging st_key / st_k / st_v nnz each (unused when n <= 1024),
+// bad one int32 (|= 1 for an index out of range).
+struct RadixPlan {
+  int rows_per_tile = 0;
+  int passes = 0;
+  int bits1 = 0;  // bits of the first digit
+  int64_t ntiles_rows = 0, ntiles_flat = 0;
+};
+bool transpose_radix_plan(int64_t m, int64_t n, int64_t nnz, RadixPlan* p);
+int64_t radix_hist_elems(const RadixPlan& p);
+cudaError_t launch_transpose_radix(const RadixPlan& p, int64_t m, int64_t n, int64_t nnz, const int64_t* rp,
+                                   const int32_t* col, const float* val, const int32_t* order, int64_t* hist,
+                                   int64_t* off, int64_t* scan_tmp, int32_t* colcnt, int64_t* colcnt64,
+                                   int32_t* st_key, int32_t* st_k, float* st_v, int32_t* bad, int64_t* cp,
+                                   int32_t* trow, float* tval, cudaStream_t s);
+
+// Deterministic CSR -> CSC (rows ascending in the order `order`, or
+// natural order when null, within each column).  cnt holds B*n int32,
+// colcount n int64, scan_tmp scan_temp_elems(n) int64, bad one int32 that
+// is set when an index is out of range.
+int transpose_blocks(int64_t m, int64_t n);
+cudaError_t launch_transpose_blocked(int64_t m, int64_t n, int B, const int64_t* rp, const int32_t* col,
+                                     const float* val, const int32_t* order, bool positions, int32_t* cnt,
+                                     int64_t* colcount, int64_t* scan_tmp, int32_t* bad, int64_t* cp, int32_t* trow,
+                                     float* tval, cudaStream_t s);
 // e_i = y_i / (A x)_i (0 for y_i == 0); optional FP64 log-likelihood sums.
 cudaError_t launch_mlem_forward(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const float* y,
-                                const float* x, float* e, double* d_ll, cudaStream_t s);
+                                const float* x, const int32_t* rank, float* e, double* d_ll, cudaStream_t s);
 // c_j = (A^T e)_j by columns; with update: out = x*c/(s+(s==0)), d_acc += sum.
 cudaError_t launch_mlem_back(int64_t n, const int64_t* cp, const int32_t* trow, const float* tval, const float* e,
                              const float* x, const float* sens, float* out, double* d_acc, bool update,

@@ -6,6 +6,7 @@
 // image x (a few MB) stays in L2, and back projection accumulates with
 // fire-and-forget float reductions (red.global.add.f32) into the image,
 // which is also L2-resident.
+#include <algorithm>
 #include <cstdint>
 
 #include "internal.h"
@@ -85,6 +86,38 @@ __device__ __forceinline__ float row_dot(const int32_t* __restrict__ col, const 
   return warp_sum((acc + acc1) + (acc2 + acc3));
 }
 
+// Dot product of CSR row [b, e) with x, one warp, lanes on consecutive
+// entries: each step loads U entries per lane (32*U consecutive entries per
+// warp, coalesced, streamed past the caches) and then gathers x for all of
+// them; one gather instruction covers 32 neighbouring columns of the row,
+// which sit in few cache lines because a row's voxels are sorted.
+template <int U>
+__device__ __forceinline__ float row_dot_seq(const int32_t* __restrict__ col, const float* __restrict__ val, int64_t b,
+                                             int64_t e, const float* __restrict__ x, int lane) {
+  static_assert(U % 4 == 0, "U is a multiple of 4");
+  float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+  const int64_t nfull = (e - b) / (32 * U);
+  int64_t k = b + lane;
+  for (int64_t i = 0; i < nfull; i++, k += 32 * U) {
+    int c[U];
+    float v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      c[u] = __ldcs(col + k + 32 * u);
+      v[u] = __ldcs(val + k + 32 * u);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u += 4) {
+      acc0 += v[u] * __ldg(x + c[u]);
+      acc1 += v[u + 1] * __ldg(x + c[u + 1]);
+      acc2 += v[u + 2] * __ldg(x + c[u + 2]);
+      acc3 += v[u + 3] * __ldg(x + c[u + 3]);
+    }
+  }
+  for (; k < e; k += 32) acc0 += __ldcs(val + k) * __ldg(x + __ldcs(col + k));
+  return warp_sum((acc0 + acc1) + (acc2 + acc3));
+}
+
 // y[col] += f * val over CSR row [b, e), by one warp.  Streaming loads:
 // this is the last use of the row in the pass.
 template <bool VEC>
@@ -112,7 +145,6 @@ __device__ __forceinline__ void row_scatter(const int32_t* __restrict__ col, con
   if (t < e) atomicAdd(y + __ldcs(col + t), __ldcs(val + t) * f);
 }
 
-template <bool VEC>
 __global__ void __launch_bounds__(kThreads) spmv_n_kernel(int64_t m, const int64_t* __restrict__ rp,
                                                           const int32_t* __restrict__ col,
                                                           const float* __restrict__ val, float alpha,
@@ -121,7 +153,7 @@ __global__ void __launch_bounds__(kThreads) spmv_n_kernel(int64_t m, const int64
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
   for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
-    float d = row_dot<VEC>(col, val, rp[r], rp[r + 1], x, lane);
+    float d = row_dot_seq<8>(col, val, rp[r], rp[r + 1], x, lane);
     if (lane == 0) y[r] = (beta == 0.f) ? alpha * d : alpha * d + beta * y[r];
   }
 }
@@ -258,57 +290,144 @@ __global__ void mlem_normalise_kernel(int64_t n, float* __restrict__ x, const fl
 
 // ---- transpose (CSC) and the two-pass MLEM iteration ------------------------
 
-__global__ void colcount_kernel(int64_t nnz, const int32_t* __restrict__ col, int32_t* __restrict__ cnt) {
-  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < nnz; k += int64_t(gridDim.x) * blockDim.x)
-    atomicAdd(cnt + __ldcs(col + k), 1);
+// Deterministic transpose.  The rows, taken in a given order (k -> row
+// order[k], or k itself), are cut into B contiguous blocks, one warp each.
+// Pass 1 counts the entries of every (column, block) pair, pass 2 turns the
+// counts of each column into exclusive offsets over the blocks, and pass 3
+// has every warp walk its rows in order and append each entry at its
+// (column, block) cursor, with a warp barrier between rows.  Within a column
+// the entries therefore come out in the order of k, whatever the
+// scheduling.  cnt is column-major (cnt[j*B + b]).  Entries with a column
+// outside [0, n) or an order entry outside [0, m) are skipped and flagged.
+__device__ __forceinline__ int64_t block_begin(int64_t m, int B, int b) { return m * b / B; }
+
+__global__ void __launch_bounds__(kThreads) tblock_count_kernel(int64_t m, int64_t n, int B,
+                                                                const int64_t* __restrict__ rp,
+                                                                const int32_t* __restrict__ col,
+                                                                const int32_t* __restrict__ order,
+                                                                int32_t* __restrict__ cnt, int32_t* __restrict__ bad) {
+  const int lane = threadIdx.x & 31;
+  const int nw = int((int64_t(gridDim.x) * blockDim.x) >> 5);
+  for (int b = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5); b < B; b += nw) {
+    const int64_t k1 = block_begin(m, B, b + 1);
+    for (int64_t k = block_begin(m, B, b); k < k1; k++) {
+      const int64_t r = order ? int64_t(__ldg(order + k)) : k;
+      if (r < 0 || r >= m) {
+        if (lane == 0) atomicOr(bad, 1);
+        continue;
+      }
+      const int64_t e = rp[r + 1];
+      for (int64_t q = rp[r] + lane; q < e; q += 32) {
+        const int j = __ldcs(col + q);
+        if (j < 0 || j >= n) {
+          atomicOr(bad, 1);
+          continue;
+        }
+        atomicAdd(cnt + int64_t(j) * B + b, 1);
+      }
+    }
+  }
 }
 
-__global__ void widen_kernel(int64_t n, const int32_t* __restrict__ a, int64_t* __restrict__ b) {
-  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
-    b[k] = a[k];
-}
-
-// Places entry (r, j) of the CSR matrix at the next free slot of column j.
-__global__ void __launch_bounds__(kThreads) transpose_fill_kernel(int64_t m, const int64_t* __restrict__ rp,
-                                                                  const int32_t* __restrict__ col,
-                                                                  const float* __restrict__ val,
-                                                                  unsigned long long* __restrict__ cursor,
-                                                                  int32_t* __restrict__ trow,
-                                                                  float* __restrict__ tval) {
+// One warp per column: cnt[j*B .. j*B+B) becomes its exclusive prefix sum,
+// colcount[j] the column total.
+__global__ void __launch_bounds__(kThreads) tblock_scan_kernel(int64_t n, int B, int32_t* __restrict__ cnt,
+                                                               int64_t* __restrict__ colcount) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
-    const int64_t b = rp[r], e = rp[r + 1];
-    for (int64_t k = b + lane; k < e; k += 32) {
-      const int j = __ldcs(col + k);
-      const unsigned long long p = atomicAdd(cursor + j, 1ull);
-      trow[p] = int32_t(r);
-      tval[p] = __ldcs(val + k);
+  for (int64_t j = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; j < n; j += nw) {
+    int32_t* c = cnt + j * B;
+    int run = 0;
+    for (int b0 = 0; b0 < B; b0 += 32) {
+      const int v = (b0 + lane < B) ? c[b0 + lane] : 0;
+      int x = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (b0 + lane < B) c[b0 + lane] = run + x - v;
+      run += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0) colcount[j] = run;
+  }
+}
+
+// Pass 3: entry (row order[k], j) goes to cp[j] + cursor(j, block of k);
+// its row id is k when POSITIONS, else the row itself.
+template <bool POSITIONS>
+__global__ void __launch_bounds__(kThreads) tblock_fill_kernel(int64_t m, int64_t n, int B,
+                                                               const int64_t* __restrict__ rp,
+                                                               const int32_t* __restrict__ col,
+                                                               const float* __restrict__ val,
+                                                               const int32_t* __restrict__ order,
+                                                               const int64_t* __restrict__ cp,
+                                                               int32_t* __restrict__ cur, int32_t* __restrict__ trow,
+                                                               float* __restrict__ tval) {
+  const int lane = threadIdx.x & 31;
+  const int nw = int((int64_t(gridDim.x) * blockDim.x) >> 5);
+  for (int b = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5); b < B; b += nw) {
+    const int64_t k1 = block_begin(m, B, b + 1);
+    for (int64_t k = block_begin(m, B, b); k < k1; k++) {
+      const int64_t r = order ? int64_t(__ldg(order + k)) : k;
+      if (r >= 0 && r < m) {
+        const int32_t id = int32_t(POSITIONS ? k : r);
+        const int64_t e = rp[r + 1];
+        // four entries per lane in flight; a row's columns are distinct, so
+        // their cursors are too
+        for (int64_t q = rp[r] + lane; q < e; q += 128) {
+          int j[4];
+          float v[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int64_t qq = q + 32 * u;
+            j[u] = -1;
+            if (qq < e) {
+              j[u] = __ldcs(col + qq);
+              v[u] = __ldcs(val + qq);
+              if (j[u] >= n) j[u] = -1;
+            }
+          }
+          int64_t pos[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (j[u] >= 0) pos[u] = cp[j[u]] + atomicAdd(cur + int64_t(j[u]) * B + b, 1);
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (j[u] >= 0) {
+              trow[pos[u]] = id;
+              tval[pos[u]] = v[u];
+            }
+        }
+      }
+      __syncwarp();
     }
   }
 }
 
 // Forward projection with the ratio: e_i = y_i / <a_i, x> for measured rows
-// (y_i != 0), e_i = 0 otherwise.
-template <bool VEC>
+// (y_i != 0), e_i = 0 otherwise.  With rank, e_i is stored at rank[i] (the
+// layout a transpose in that order reads).
 __global__ void __launch_bounds__(kThreads) mlem_forward_kernel(int64_t m, const int64_t* __restrict__ rp,
                                                                 const int32_t* __restrict__ col,
                                                                 const float* __restrict__ val,
                                                                 const float* __restrict__ y,
-                                                                const float* __restrict__ x, float* __restrict__ e,
-                                                                double* __restrict__ ll) {
+                                                                const float* __restrict__ x,
+                                                                const int32_t* __restrict__ rank,
+                                                                float* __restrict__ e, double* __restrict__ ll) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
   double ly = 0.0, lt = 0.0;
   for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
     const float yi = __ldg(y + r);
+    const int64_t dst = rank ? int64_t(__ldg(rank + r)) : r;
     if (yi == 0.f) {
-      if (lane == 0) e[r] = 0.f;
+      if (lane == 0) e[dst] = 0.f;
       continue;
     }
-    const float yt = row_dot<VEC>(col, val, rp[r], rp[r + 1], x, lane);
+    const float yt = row_dot_seq<8>(col, val, rp[r], rp[r + 1], x, lane);
     if (lane == 0) {
-      e[r] = __fdiv_rn(yi, yt);
+      e[dst] = __fdiv_rn(yi, yt);
       if (ll) {
         ly += double(yi) * log(double(yt));
         lt += double(yt);
@@ -378,14 +497,8 @@ cudaError_t launch_spmv(int op, int64_t m, int64_t n, const int64_t* rp, const i
                         float alpha, const float* x, float beta, float* y, cudaStream_t s) {
   if (op == RAPTR_OP_N) {
     if (m > 0) {
-      if (aligned16(col, val)) {
-        spmv_n_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, beta, y);
-        note_launches(1);
-      }
-      else {
-        spmv_n_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, beta, y);
-        note_launches(1);
-      }
+      spmv_n_kernel<<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, alpha, x, beta, y);
+      note_launches(1);
     }
   } else {
     if (beta != 1.f && n > 0) {
@@ -507,42 +620,46 @@ cudaError_t launch_mlem_normalise_from(int64_t n, float* x, const float* xx, dou
   return cudaGetLastError();
 }
 
-cudaError_t launch_column_counts(int64_t nnz, const int32_t* col, int32_t* cnt, cudaStream_t s) {
-  if (nnz > 0) {
-    colcount_kernel<<<148 * 16, kThreads, 0, s>>>(nnz, col, cnt);
-    note_launches(1);
-  }
-  return cudaGetLastError();
+int transpose_blocks(int64_t m, int64_t n) {
+  // enough warps to fill the GPU, with the count table (B x n int32) kept
+  // under 4 GiB
+  int64_t B = (int64_t(4) << 30) / (4 * std::max<int64_t>(n, 1));
+  B = std::min<int64_t>(B, 4096);
+  B = std::max<int64_t>(B & ~int64_t(31), 32);
+  B = std::min<int64_t>(B, std::max<int64_t>(m, 1));
+  return int(B);
 }
 
-cudaError_t launch_widen(int64_t n, const int32_t* a, int64_t* b, cudaStream_t s) {
-  if (n > 0) {
-    widen_kernel<<<ew_grid(n), kThreads, 0, s>>>(n, a, b);
+cudaError_t launch_transpose_blocked(int64_t m, int64_t n, int B, const int64_t* rp, const int32_t* col,
+                                     const float* val, const int32_t* order, bool positions, int32_t* cnt,
+                                     int64_t* colcount, int64_t* scan_tmp, int32_t* bad, int64_t* cp, int32_t* trow,
+                                     float* tval, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(cnt, 0, size_t(B) * size_t(n) * sizeof(int32_t), s);
+  if (e != cudaSuccess) return e;
+  const unsigned gb = unsigned((int64_t(B) * 32 + kThreads - 1) / kThreads);
+  if (m > 0) {
+    tblock_count_kernel<<<gb, kThreads, 0, s>>>(m, n, B, rp, col, order, cnt, bad);
     note_launches(1);
   }
-  return cudaGetLastError();
-}
-
-cudaError_t launch_transpose_fill(int64_t m, const int64_t* rp, const int32_t* col, const float* val,
-                                  int64_t* cursor, int32_t* trow, float* tval, cudaStream_t s) {
-  if (m > 0)
-    transpose_fill_kernel<<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val,
-                                                           reinterpret_cast<unsigned long long*>(cursor), trow, tval);
+  tblock_scan_kernel<<<row_grid(n), kThreads, 0, s>>>(n, B, cnt, colcount);
+  note_launches(1);
+  e = launch_scan_i64(colcount, n, cp, scan_tmp, s);
+  if (e != cudaSuccess) return e;
+  if (m > 0) {
+    if (positions)
+      tblock_fill_kernel<true><<<gb, kThreads, 0, s>>>(m, n, B, rp, col, val, order, cp, cnt, trow, tval);
+    else
+      tblock_fill_kernel<false><<<gb, kThreads, 0, s>>>(m, n, B, rp, col, val, order, cp, cnt, trow, tval);
     note_launches(1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_mlem_forward(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const float* y,
-                                const float* x, float* e, double* d_ll, cudaStream_t s) {
+                                const float* x, const int32_t* rank, float* e, double* d_ll, cudaStream_t s) {
   if (m > 0) {
-    if (aligned16(col, val)) {
-      mlem_forward_kernel<true><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, e, d_ll);
-      note_launches(1);
-    }
-    else {
-      mlem_forward_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, e, d_ll);
-      note_launches(1);
-    }
+    mlem_forward_kernel<<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, rank, e, d_ll);
+    note_launches(1);
   }
   return cudaGetLastError();
 }

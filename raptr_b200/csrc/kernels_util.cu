@@ -166,6 +166,70 @@ cudaError_t launch_widen_i32(const int32_t* in, int64_t n, int64_t* out, cudaStr
   return cudaGetLastError();
 }
 
+// ---- back-projection order of channels ------------------------------------
+//
+// A channel joins crystal (z0, y0) of head 0 to (z1, y1) of head 1.  Sorting
+// channels by (angle, z0+z1, y0+y1, z0-z1, y0-y1) groups lines by their
+// midpoint before their slope, so the channels that cross one voxel sit in
+// few short runs: a column of the transpose then reads a vector laid out in
+// this order in dense runs instead of scattered words.
+__device__ __forceinline__ int64_t channel_order_key(const DGeom& g, int cnl) {
+  const ChannelIds c = channel_split(g, cnl);
+  const int64_t sz = g.n0z + g.n1z - 1, sy = g.n0y + g.n1y - 1;
+  int64_t k = c.ida;
+  k = k * sz + (c.id0z + c.id1z);
+  k = k * sy + (c.id0y + c.id1y);
+  k = k * sz + (c.id0z - c.id1z + g.n1z - 1);
+  k = k * sy + (c.id0y - c.id1y + g.n1y - 1);
+  return k;
+}
+
+__global__ void order_mark_kernel(DGeom g, int64_t m, const int32_t* __restrict__ cnl, int64_t nkeys,
+                                  unsigned long long* __restrict__ mark, int32_t* __restrict__ bad) {
+  const int64_t nch = int64_t(g.na) * g.n0z * g.n0y * g.n1z * g.n1y;
+  for (int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < m; r += int64_t(gridDim.x) * blockDim.x) {
+    const int c = cnl[r];
+    if (c < 0 || c >= nch) {
+      atomicOr(bad, 1);
+      continue;
+    }
+    const int64_t k = channel_order_key(g, c);
+    if (k < 0 || k >= nkeys || atomicAdd(mark + k, 1ull) != 0ull) atomicOr(bad, 1);
+  }
+}
+
+__global__ void order_rank_kernel(DGeom g, int64_t m, const int32_t* __restrict__ cnl,
+                                  const int64_t* __restrict__ prefix, int32_t* __restrict__ rank,
+                                  int32_t* __restrict__ order) {
+  for (int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < m; r += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t k = prefix[channel_order_key(g, cnl[r])];
+    rank[r] = int32_t(k);
+    order[k] = int32_t(r);
+  }
+}
+
+int64_t channel_order_keys(const DGeom& g) {
+  const int64_t sz = g.n0z + g.n1z - 1, sy = g.n0y + g.n1y - 1;
+  return int64_t(g.na) * sz * sz * sy * sy;
+}
+
+cudaError_t launch_channel_order_mark(const DGeom& g, int64_t m, const int32_t* cnl, unsigned long long* mark,
+                                      int32_t* bad, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(mark, 0, size_t(channel_order_keys(g)) * sizeof(unsigned long long), s);
+  if (e != cudaSuccess || m <= 0) return e;
+  order_mark_kernel<<<grid_for(m, 256), 256, 0, s>>>(g, m, cnl, channel_order_keys(g), mark, bad);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_channel_order_rank(const DGeom& g, int64_t m, const int32_t* cnl, const int64_t* prefix,
+                                      int32_t* rank, int32_t* order, cudaStream_t s) {
+  if (m <= 0) return cudaSuccess;
+  order_rank_kernel<<<grid_for(m, 256), 256, 0, s>>>(g, m, cnl, prefix, rank, order);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
 int64_t scan_temp_elems(int64_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
 
 cudaError_t launch_scan_i64(const int64_t* in, int64_t n, int64_t* out, int64_t* temp, cudaStream_t s) {

@@ -322,24 +322,84 @@ def test_mlem_matches_oracle(rlib, oracle, torch, ctx_small, small_full_matrix, 
         assert np.all(np.diff(ll) >= -1e-6 * abs(ll[-1]))  # MLEM never decreases the likelihood
 
 
+def channel_order_keys(g, cnl):
+    """Back-projection order key of channels: (angle, z0+z1, y0+y1, z0-z1,
+    y0-y1), y1 fastest in the channel id."""
+    c = np.asarray(cnl, np.int64)
+    y1 = c % g.n1y
+    z1 = (c // g.n1y) % g.n1z
+    y0 = (c // (g.n1y * g.n1z)) % g.n0y
+    z0 = (c // (g.n1y * g.n1z * g.n0y)) % g.n0z
+    a = c // (g.n1y * g.n1z * g.n0y * g.n0z)
+    sz, sy = g.n0z + g.n1z - 1, g.n0y + g.n1y - 1
+    return (((a * sz + z0 + z1) * sy + y0 + y1) * sz + z0 - z1 + g.n1z - 1) * sy + y0 - y1 + g.n1y - 1
+
+
+def csc_reference(m, n, rp, col, val):
+    """CSC with rows ascending within each column (numpy stable sort)."""
+    rows = np.repeat(np.arange(m), np.diff(rp))
+    o = np.argsort(col, kind="stable")
+    cp = np.zeros(n + 1, np.int64)
+    cp[1:] = np.cumsum(np.bincount(col, minlength=n))
+    return cp, rows[o].astype(np.int32), val[o]
+
+
 def test_transpose_is_csc_of_the_matrix(rlib, torch, small_full_matrix):
-    A, _, _ = small_full_matrix
+    A, _, lst = small_full_matrix
     A.transpose()
     rp, col, val = A.to_numpy()
     cp = A.col_ptr.cpu().numpy()
     ri = A.row_idx.cpu().numpy()
     tv = A.tval.cpu().numpy()
-    assert cp[0] == 0 and cp[-1] == A.nnz and np.all(np.diff(cp) == np.bincount(col, minlength=A.n))
-    # same entries: sort both by (column, row)
-    rows = np.repeat(np.arange(A.m), np.diff(rp))
-    a = np.lexsort((rows, col))
-    tcol = np.repeat(np.arange(A.n), np.diff(cp))
-    b = np.lexsort((ri, tcol))
-    assert np.array_equal(rows[a], ri[b]) and np.array_equal(col[a], tcol[b])
-    assert np.array_equal(val[a].view(np.uint32), tv[b].view(np.uint32))
-    # the caller-buffer variant agrees
-    cp2, ri2, tv2 = rlib.csr_transpose(A.m, A.n, A.row_ptr, A.col, A.val)
-    assert np.array_equal(cp2.cpu().numpy(), cp)
+    # the rows come in the back-projection order of their channels
+    order = A.row_order.cpu().numpy()
+    rank = A.row_rank.cpu().numpy()
+    assert np.array_equal(order, np.argsort(channel_order_keys(cfg.SMALL, lst), kind="stable"))
+    assert np.array_equal(rank[order], np.arange(A.m))
+    # positions ascend within each column, and mapped back to rows the
+    # transpose is exactly the CSC of the matrix in that order
+    pos_rows = rank[np.repeat(np.arange(A.m), np.diff(rp))]
+    o = np.lexsort((pos_rows, col))
+    assert np.array_equal(cp, np.concatenate([[0], np.cumsum(np.bincount(col, minlength=A.n))]))
+    assert np.array_equal(ri, pos_rows[o])
+    assert np.array_equal(tv.view(np.uint32), val[o].view(np.uint32))
+    assert np.array_equal(order[ri], np.repeat(np.arange(A.m), np.diff(rp))[o])
+
+
+def test_csr_transpose_is_deterministic_and_sorted(rlib, torch, small_full_matrix):
+    A, _, _ = small_full_matrix
+    rp, col, val = A.to_numpy()
+    cp_ref, ri_ref, tv_ref = csc_reference(A.m, A.n, rp, col, val)
+    for _ in range(2):
+        cp, ri, tv = rlib.csr_transpose(A.m, A.n, A.row_ptr, A.col, A.val)
+        assert np.array_equal(cp.cpu().numpy(), cp_ref)
+        assert np.array_equal(ri.cpu().numpy(), ri_ref)
+        assert np.array_equal(tv.cpu().numpy().view(np.uint32), tv_ref.view(np.uint32))
+
+
+def test_csr_transpose_in_a_given_order(rlib, torch, small_full_matrix):
+    A, _, _ = small_full_matrix
+    rp, col, val = A.to_numpy()
+    order = np.random.default_rng(5).permutation(A.m).astype(np.int32)
+    rank = np.empty(A.m, np.int64)
+    rank[order] = np.arange(A.m)
+    cp, pos, tv = rlib.csr_transpose_ordered(A.m, A.n, A.row_ptr, A.col, A.val, torch.from_numpy(order).cuda())
+    pos_rows = rank[np.repeat(np.arange(A.m), np.diff(rp))]
+    o = np.lexsort((pos_rows, col))
+    assert np.array_equal(pos.cpu().numpy(), pos_rows[o])
+    assert np.array_equal(tv.cpu().numpy().view(np.uint32), val[o].view(np.uint32))
+    # back projection through it reads e in that order
+    e = torch.rand(A.m, device="cuda")
+    c_nat = rlib.spmv(rlib.OP_T, A.m, A.n, A.row_ptr, A.col, A.val, e)
+    c = torch.zeros(A.n, device="cuda")
+    rlib.lib().raptr_mlem_back(A.n, cp.data_ptr(), pos.data_ptr(), tv.data_ptr(),
+                               e[torch.from_numpy(order).long().cuda()].contiguous().data_ptr(), c.data_ptr(), None)
+    assert torch.allclose(c, c_nat, rtol=1e-5, atol=1e-6 * float(c_nat.abs().max()))
+    # a bad order entry is an error, not a fault
+    bad = order.copy()
+    bad[3] = A.m + 7
+    with pytest.raises(RuntimeError):
+        rlib.csr_transpose_ordered(A.m, A.n, A.row_ptr, A.col, A.val, torch.from_numpy(bad).cuda())
 
 
 def test_mlem_half_steps_equal_full_iteration(rlib, torch, ctx_small, small_full_matrix, small_measurement):
