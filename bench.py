@@ -58,6 +58,7 @@ def parse_args():
     p.add_argument("--workload", choices=list(cfg.WORKLOADS), default="full")
     p.add_argument("--cpu-sample-s", type=float, default=12.0, help="CPU seconds for the cpu_baseline sample")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-forms", action="store_true", help="skip the FP16 / batched / serving forms")
     return p.parse_args()
 
 
@@ -318,6 +319,69 @@ def run_job(R, torch, ctx, w, lst, y_dev, dist=None):
             "kernel_ms": kt, "x": x, **info}
 
 
+def precision_report(R, torch, ctx, w, lst, y_dev, peak):
+    """The FP16-matrix form beside the FP32 one, both against the FP64
+    iteration on the same matrix: relative L2 and max error of the image
+    after 10 / 25 / 50 iterations, iteration rates (CUDA graph) and the
+    roofline of the FP16 passes."""
+    g = w["geom"]
+    n = g.n_voxels
+    A = ctx.build(lst, w["nrays"], SEED)
+    A.transpose()
+    A.to_half()
+    nnz, m = A.nnz, A.m
+    s64, s32 = R.sensitivity(A)
+    h64, h32 = R.sensitivity_half(A)
+    marks = [c for c in (10, 25, 50) if c <= w["niter"]] or [w["niter"]]
+    x64 = torch.full((n,), 1.0 / n, dtype=torch.float64, device="cuda")
+    x32 = torch.full((n,), np.float32(1.0 / n), device="cuda")
+    x16 = torch.full((n,), np.float32(1.0 / n), device="cuda")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    errs = {"fp32": {}, "fp16": {}}
+    ms = {"fp32": 0.0, "fp16": 0.0}
+    kt16 = []
+    done = 0
+    for mark in marks:
+        k = mark - done
+        ctx.mlem_f64(A, y_dev, s64 / s64.sum(), x64, k)
+        ev[0].record()
+        ctx.mlem(A, y_dev, s32, x32, k, use_graph=True)
+        ev[1].record()
+        ctx.mlem_half(A, y_dev, h32, x16, k, use_graph=True)
+        ev[2].record()
+        torch.cuda.synchronize()
+        ms["fp32"] += ev[0].elapsed_time(ev[1])
+        ms["fp16"] += ev[1].elapsed_time(ev[2])
+        ref = x64
+        for name, x in (("fp32", x32), ("fp16", x16)):
+            d = x.double() - ref
+            errs[name][str(mark)] = {"rel_l2": float(d.norm() / ref.norm()),
+                                     "max_rel": float(d.abs().max() / ref.abs().max())}
+        done = mark
+    # per-pass device times of the FP16 iteration (no graph, events between passes)
+    kt16 = ctx.mlem_half(A, y_dev, h32, x16.clone(), 5, use_graph=False, kernel_times=True)
+    fwd_ms, back_ms = float(kt16[:, 0].mean()), float(kt16[:, 1].mean())
+    fwd_b = nnz * 6 + (m + 1) * 8 + m * 4 * 4 + n * 4
+    back_b = nnz * 6 + (n + 1) * 8 + 3 * n * 4 + m * 4
+    out = {
+        "iterations": done,
+        "iters_per_s": {k: done / (v / 1e3) for k, v in ms.items()},
+        "speedup_fp16_vs_fp32": ms["fp32"] / ms["fp16"],
+        "error_vs_fp64": errs,
+        "matrix_bytes_per_entry": {"fp32": 8, "fp16": 6},
+        "roofline_fp16": {
+            "mlem_forward_half_kernel": {"achieved": round(fwd_b / fwd_ms / 1e6, 1),
+                                         "frac": round(fwd_b / fwd_ms / 1e6 / peak, 4), "ms": round(fwd_ms, 4)},
+            "mlem_back_half_kernel": {"achieved": round(back_b / back_ms / 1e6, 1),
+                                      "frac": round(back_b / back_ms / 1e6 / peak, 4), "ms": round(back_ms, 4)},
+        },
+        "reference": "FP64 vectors and accumulation over the FP32 matrix (raptr_mlem_f64, GPU)",
+    }
+    del A
+    gc.collect()
+    return out
+
+
 def main():
     args = parse_args()
     w = workload(args.workload)
@@ -464,6 +528,9 @@ def main():
         out["e2e"] = {"value": w["niter"] / e2e_s, "unit": "MLEM iterations/s",
                       "h2d_bytes_per_step": int(st["h2d_bytes"]), "d2h_bytes_per_step": int(st["d2h_bytes"]),
                       "wall_s": e2e_s, "build_ms": st["build_ms"], "iter_ms": st["iter_ms"]}
+    if rank == 0 and world == 1 and not args.no_forms:
+        peak, _ = measured_peaks()
+        out["forms"] = {"precision": precision_report(R, torch, ctx, w, lst, y_dev, peak)}
     if rank == 0 and world == 1:
         out["cpu_baseline"] = {k: v for k, v in cpu_job_rate(w, args.cpu_sample_s, os.cpu_count() or 1).items()
                                if k != "matrix_build_s"}

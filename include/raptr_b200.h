@@ -270,6 +270,67 @@ raptr_status raptr_mlem_forward_ordered(int64_t m, const int64_t* d_row_ptr, con
                                         const float* d_y, const float* d_x, const int32_t* d_row_rank, float* d_e,
                                         double* d_ll, void* stream);
 
+/* ---- precision forms ------------------------------------------------------
+ * No counterpart in the reference (FP32 throughout, src/tests/reco.cu).
+ *
+ * FP16 system matrix: a_ij ~= rscale_i * h_ij with h IEEE binary16 (as
+ * uint16_t bits) and rscale_i = max_j |a_ij| * 2^-15, so h <= 32768.  The
+ * matrix keeps h in CSR order (d_hval) and in the order of its transpose
+ * (d_htval), and the row scales by row (d_rscale) and by position of the
+ * transpose (d_pscale).  Requires raptr_matrix_transpose; synchronises. */
+raptr_status raptr_matrix_half(raptr_matrix* A, void* stream);
+raptr_status raptr_matrix_half_info(const raptr_matrix* A, uint16_t** d_hval, float** d_rscale, uint16_t** d_htval,
+                                    float** d_pscale);
+/* FP64 column sums of the FP16 matrix (through its transpose), and the same
+ * normalised to sum 1 in float when d_s32 is non-null. */
+raptr_status raptr_sensitivity_half(int64_t n, const int64_t* d_col_ptr, const int32_t* d_row_idx,
+                                    const uint16_t* d_htval, const float* d_pscale, double* d_s64, float* d_s32,
+                                    void* stream);
+/* raptr_mlem with the FP16 matrix: FP32 vectors and accumulation, the back
+ * projection's compensated; the transpose is required (opts->d_row_rank as
+ * for raptr_mlem).  Per entry 6 matrix bytes per pass instead of 8. */
+raptr_status raptr_mlem_half(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                             const uint16_t* d_hval, const float* d_rscale, const int64_t* d_col_ptr,
+                             const int32_t* d_row_idx, const uint16_t* d_htval, const float* d_y, const float* d_s,
+                             float* d_x, int32_t n_iter, const raptr_mlem_opts* opts, void* stream);
+/* The same iteration with FP64 vectors and accumulation over the FP32
+ * matrix (the reference for the FP32 and FP16 images): d_s64 is the
+ * normalised sensitivity, d_x64 the image (updated in place); h_loglik,
+ * when non-null, receives n_iter log-likelihoods.  Synchronises. */
+raptr_status raptr_mlem_f64(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                            const float* d_val, const int64_t* d_col_ptr, const int32_t* d_row_idx,
+                            const float* d_tval, const int32_t* d_row_rank, const float* d_y, const double* d_s64,
+                            double* d_x64, int32_t n_iter, double* h_loglik, void* stream);
+
+/* ---- batched frames -------------------------------------------------------
+ * No counterpart in the reference (one measurement per run).  n_frames
+ * reconstructions that share one system matrix, iterated together: d_y
+ * (m x n_frames) and d_x (n x n_frames) are frame-minor (y[i*n_frames + f]),
+ * d_s is the one normalised sensitivity; each frame's image is normalised
+ * to sum 1 after every iteration.  The matrix is FP32 (value_type 0: d_val /
+ * d_tval float) or the FP16 form (value_type 1: d_val = hval, d_tval =
+ * htval, d_rscale the row scales); the transpose is required and d_row_rank
+ * follows it (raptr_matrix_row_order, may be null for the natural order).
+ * Each pass handles frame_tile frames per sweep of the matrix (4, 8, 16, 32
+ * or 64, dividing n_frames; 0 = the default 32-or-smaller divisor).
+ * opts: use_graph captures the n_iter iterations in a CUDA graph;
+ * h_kernel_ms receives per iteration the forward and back-pass times. */
+raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_frames, int32_t value_type,
+                              const int64_t* d_row_ptr, const int32_t* d_col, const void* d_val,
+                              const float* d_rscale, const int64_t* d_col_ptr, const int32_t* d_row_idx,
+                              const void* d_tval, const int32_t* d_row_rank, const float* d_y, const float* d_s,
+                              float* d_x, int32_t n_iter, int32_t frame_tile, const raptr_mlem_opts* opts,
+                              void* stream);
+/* Picks the frame tile by timing one iteration per candidate on a copy of
+ * d_x (left unchanged): *best_tile, and h_ms[5] (when non-null) the times
+ * for tiles 4, 8, 16, 32, 64 (-1 where the tile does not divide n_frames). */
+raptr_status raptr_mlem_batch_autotune(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_frames, int32_t value_type,
+                                       const int64_t* d_row_ptr, const int32_t* d_col, const void* d_val,
+                                       const float* d_rscale, const int64_t* d_col_ptr, const int32_t* d_row_idx,
+                                       const void* d_tval, const int32_t* d_row_rank, const float* d_y,
+                                       const float* d_s, const float* d_x, int32_t* best_tile, float* h_ms,
+                                       void* stream);
+
 /* MLEM iterations that allocate no device memory.  No counterpart in the
  * reference (which allocates its buffers itself).  For callers that cannot
  * allocate where they reconstruct -- e.g. a server that reserves its whole

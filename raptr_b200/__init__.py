@@ -121,6 +121,16 @@ _SIGNATURES = {
     "raptr_matrix_transpose": (C.c_int, [VP, VP]),
     "raptr_matrix_csc_info": (C.c_int, [VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP)]),
     "raptr_matrix_row_order": (C.c_int, [VP, C.POINTER(VP), C.POINTER(VP)]),
+    "raptr_matrix_half": (C.c_int, [VP, VP]),
+    "raptr_matrix_half_info": (C.c_int, [VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), C.POINTER(VP)]),
+    "raptr_sensitivity_half": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, VP]),
+    "raptr_mlem_half": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32,
+                                  C.POINTER(raptr_mlem_opts), VP]),
+    "raptr_mlem_f64": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32, VP, VP]),
+    "raptr_mlem_batch": (C.c_int, [VP, I64, I64, I32, I32, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32, I32,
+                                   C.POINTER(raptr_mlem_opts), VP]),
+    "raptr_mlem_batch_autotune": (C.c_int, [VP, I64, I64, I32, I32, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP,
+                                            C.POINTER(C.c_int32), C.POINTER(C.c_float), VP]),
     "raptr_csr_transpose": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_csr_transpose_ordered": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_mlem_noalloc": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, I32, VP]),
@@ -252,6 +262,30 @@ class Matrix:
             self.row_rank = torch.as_tensor(_DeviceArray(rank.value, (self.m,), "<i4", own), device=dev)
         return self
 
+    # FP16 form (to_half): h values in CSR and transpose order, row scales
+    hval = None
+    rscale = None
+    htval = None
+    pscale = None
+
+    def to_half(self, stream=None) -> "Matrix":
+        """Builds the FP16 copy (a_ij ~= rscale_i * h_ij) beside the FP32
+        matrix; transposes first if needed."""
+        if not self.has_transpose:
+            self.transpose(stream)
+        _check(lib().raptr_matrix_half(self._h, _stream(stream)))
+        hv, rs, ht, ps = VP(), VP(), VP(), VP()
+        _check(lib().raptr_matrix_half_info(self._h, C.byref(hv), C.byref(rs), C.byref(ht), C.byref(ps)))
+        torch = _torch()
+        dev = torch.device("cuda", self.device)
+        own = self._owner
+        nz, mm = max(self.nnz, 1), max(self.m, 1)
+        self.hval = torch.as_tensor(_DeviceArray(hv.value, (nz,), "<f2", own), device=dev)[:self.nnz]
+        self.htval = torch.as_tensor(_DeviceArray(ht.value, (nz,), "<f2", own), device=dev)[:self.nnz]
+        self.rscale = torch.as_tensor(_DeviceArray(rs.value, (mm,), "<f4", own), device=dev)[:self.m]
+        self.pscale = torch.as_tensor(_DeviceArray(ps.value, (mm,), "<f4", own), device=dev)[:self.m]
+        return self
+
     def to_numpy(self):
         return self.row_ptr.cpu().numpy(), self.col.cpu().numpy(), self.val.cpu().numpy()
 
@@ -364,7 +398,84 @@ class Context:
         return None if not out else (out[0] if len(out) == 1 else tuple(out))
 
 
+    def mlem_half(self, A: Matrix, y, s, x, niter: int, use_graph: bool = True, loglik: bool = False,
+                  kernel_times: bool = False, stream=None):
+        """MLEM iterations with A's FP16 copy (A.to_half()); as mlem()."""
+        assert A.hval is not None, "call A.to_half() first"
+        ll = (C.c_double * max(niter, 1))() if loglik else None
+        kt = (C.c_float * max(2 * niter, 1))() if kernel_times else None
+        opts = raptr_mlem_opts(1 if use_graph else 0, C.cast(ll, C.POINTER(C.c_double)) if loglik else None,
+                               C.cast(kt, C.POINTER(C.c_float)) if kernel_times else None, _ptr(A.row_rank))
+        _check(lib().raptr_mlem_half(self._h, A.m, A.n, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.hval),
+                                     _ptr(A.rscale), _ptr(A.col_ptr), _ptr(A.row_idx), _ptr(A.htval), _ptr(y),
+                                     _ptr(s), _ptr(x), niter, C.byref(opts), _stream(stream)))
+        out = []
+        if loglik:
+            out.append(np.array(ll[:niter]))
+        if kernel_times:
+            out.append(np.array(kt[:2 * niter], np.float64).reshape(niter, 2))
+        return None if not out else (out[0] if len(out) == 1 else tuple(out))
+
+    def _batch_arrays(self, A: Matrix, half: bool):
+        if not A.has_transpose:
+            A.transpose()
+        if half:
+            if A.hval is None:
+                A.to_half()
+            return 1, _ptr(A.hval), _ptr(A.rscale), _ptr(A.htval)
+        return 0, _ptr(A.val), None, _ptr(A.tval)
+
+    def mlem_batch(self, A: Matrix, Y, s, X, niter: int, frame_tile: int = 0, half: bool = True,
+                   use_graph: bool = True, kernel_times: bool = False, stream=None):
+        """MLEM for K frames together: Y (m, K) and X (n, K) float32,
+        row-major (frame-minor); s the one normalised sensitivity.  Returns
+        the (niter, 2) pass times with kernel_times, else None."""
+        K = int(X.shape[1])
+        assert Y.shape == (A.m, K) and X.shape == (A.n, K) and X.is_contiguous() and Y.is_contiguous()
+        vt, val, rsc, tval = self._batch_arrays(A, half)
+        kt = (C.c_float * max(2 * niter, 1))() if kernel_times else None
+        opts = raptr_mlem_opts(1 if use_graph else 0, None, C.cast(kt, C.POINTER(C.c_float)) if kernel_times else None,
+                               None)
+        _check(lib().raptr_mlem_batch(self._h, A.m, A.n, K, vt, _ptr(A.row_ptr), _ptr(A.col), val, rsc,
+                                      _ptr(A.col_ptr), _ptr(A.row_idx), tval, _ptr(A.row_rank), _ptr(Y), _ptr(s),
+                                      _ptr(X), niter, frame_tile, C.byref(opts), _stream(stream)))
+        return np.array(kt[:2 * niter], np.float64).reshape(niter, 2) if kernel_times else None
+
+    def batch_autotune(self, A: Matrix, Y, s, X, half: bool = True, stream=None):
+        """(best frame tile, {tile: ms per iteration}) for these frames."""
+        K = int(X.shape[1])
+        vt, val, rsc, tval = self._batch_arrays(A, half)
+        best = C.c_int32(0)
+        ms = (C.c_float * 5)()
+        _check(lib().raptr_mlem_batch_autotune(self._h, A.m, A.n, K, vt, _ptr(A.row_ptr), _ptr(A.col), val, rsc,
+                                               _ptr(A.col_ptr), _ptr(A.row_idx), tval, _ptr(A.row_rank), _ptr(Y),
+                                               _ptr(s), _ptr(X), C.byref(best), ms, _stream(stream)))
+        return best.value, {t: float(v) for t, v in zip((4, 8, 16, 32, 64), ms) if v >= 0}
+
+    def mlem_f64(self, A: Matrix, y, s64, x64, niter: int, loglik: bool = False, stream=None):
+        """MLEM iterations with FP64 vectors (x64, s64: float64 tensors; s64
+        normalised to sum 1) over the FP32 matrix and its transpose."""
+        if not A.has_transpose:
+            A.transpose(stream)
+        ll = (C.c_double * max(niter, 1))() if loglik else None
+        _check(lib().raptr_mlem_f64(self._h, A.m, A.n, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(A.col_ptr),
+                                    _ptr(A.row_idx), _ptr(A.tval), _ptr(A.row_rank), _ptr(y), _ptr(s64), _ptr(x64),
+                                    niter, C.cast(ll, C.POINTER(C.c_double)) if loglik else None,
+                                    _stream(stream)))
+        return np.array(ll[:niter]) if loglik else None
+
+
 # -- context-free operations ---------------------------------------------------
+
+
+def sensitivity_half(A: Matrix, stream=None):
+    """(FP64 column sums of A's FP16 copy, FP32 image normalised to sum 1)."""
+    torch = _torch()
+    s64 = torch.empty(A.n, dtype=torch.float64, device=A.row_ptr.device)
+    s32 = torch.empty(A.n, dtype=torch.float32, device=A.row_ptr.device)
+    _check(lib().raptr_sensitivity_half(A.n, _ptr(A.col_ptr), _ptr(A.row_idx), _ptr(A.htval), _ptr(A.pscale),
+                                        _ptr(s64), _ptr(s32), _stream(stream)))
+    return s64, s32
 
 def spmv(op: int, m: int, n: int, row_ptr, col, val, x, alpha=1.0, beta=0.0, y=None, stream=None):
     """CSRmv: y = alpha*op(A)*x + beta*y."""

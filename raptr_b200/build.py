@@ -26,6 +26,8 @@ UNITS = {
     "kernels_util.cu": [],
     "kernels_mlem.cu": [],
     "kernels_transpose.cu": [],
+    "kernels_precision.cu": [],
+    "kernels_batch.cu": [],
     "mlem_noalloc.cu": [],
 }
 

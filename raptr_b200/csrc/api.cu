@@ -145,6 +145,11 @@ struct raptr_matrix {
   DGeom geom{};
   int32_t* rank = nullptr;   // row -> position
   int32_t* order = nullptr;  // position -> row
+  // FP16 form, built on request: a_ij ~= rscale_i * h_ij
+  float* rscale = nullptr;
+  float* pscale = nullptr;   // rscale by position of the transpose
+  uint16_t* hval = nullptr;  // CSR order
+  uint16_t* htval = nullptr; // transpose order
 };
 
 namespace {
@@ -521,6 +526,10 @@ raptr_status raptr_matrix_destroy(raptr_matrix* A) {
   cudaFree(A->cnl);
   cudaFree(A->rank);
   cudaFree(A->order);
+  cudaFree(A->rscale);
+  cudaFree(A->pscale);
+  cudaFree(A->hval);
+  cudaFree(A->htval);
   delete A;
   return RAPTR_OK;
 }
@@ -849,15 +858,34 @@ raptr_status raptr_mlem_back(int64_t n, const int64_t* d_col_ptr, const int32_t*
   return RAPTR_OK;
 }
 
-raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
-                        const float* d_val, const int64_t* d_col_ptr, const int32_t* d_row_idx, const float* d_tval,
-                        const float* d_y, const float* d_s, float* d_x, int32_t n_iter, const raptr_mlem_opts* opts,
-                        void* stream) {
-  if (!ctx || m < 0 || n <= 0 || n_iter < 0 || !d_row_ptr || !d_y || !d_s || !d_x)
-    return fail(RAPTR_ERR_INVALID, "bad argument");
+namespace {
+
+// Arrays of one MLEM form: FP16 when htval is set (with hval, rscale and
+// the transpose), FP32 gather when the transpose is given, else FP32
+// scatter over the rows.
+struct MlemArrays {
+  const int64_t* rp = nullptr;
+  const int32_t* col = nullptr;
+  const float* val = nullptr;
+  const uint16_t* hval = nullptr;
+  const float* rscale = nullptr;
+  const int64_t* cp = nullptr;
+  const int32_t* trow = nullptr;
+  const float* tval = nullptr;
+  const uint16_t* htval = nullptr;
+};
+
+raptr_status mlem_impl(raptr_ctx* ctx, int64_t m, int64_t n, const MlemArrays& A, const float* d_y, const float* d_s,
+                       float* d_x, int32_t n_iter, const raptr_mlem_opts* opts, cudaStream_t s) {
+  const int64_t* d_row_ptr = A.rp;
+  const int32_t* d_col = A.col;
+  const float* d_val = A.val;
+  const int64_t* d_col_ptr = A.cp;
+  const int32_t* d_row_idx = A.trow;
+  const float* d_tval = A.tval;
+  const bool half = A.htval != nullptr;
   if (n_iter == 0) return RAPTR_OK;
   DeviceScope ds(ctx->device);
-  cudaStream_t s = as_stream(stream);
   const bool want_ll = opts && opts->h_loglik;
   const bool want_times = opts && opts->h_kernel_ms;
   const bool use_graph = opts && opts->use_graph && !want_times;
@@ -885,9 +913,12 @@ raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_r
       if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it)], q);
       if (csc) {
         if (err == cudaSuccess)
-          err = launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, rank, e, lli, q);
+          err = half ? launch_mlem_forward_half(m, d_row_ptr, d_col, A.hval, A.rscale, d_y, d_x, rank, e, lli, q)
+                     : launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, rank, e, lli, q);
         if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 1)], q);
-        if (err == cudaSuccess) err = launch_mlem_back(n, d_col_ptr, d_row_idx, d_tval, e, d_x, d_s, c, acc, true, q);
+        if (err == cudaSuccess)
+          err = half ? launch_mlem_back_half(n, d_col_ptr, d_row_idx, A.htval, e, d_x, d_s, c, acc, true, q)
+                     : launch_mlem_back(n, d_col_ptr, d_row_idx, d_tval, e, d_x, d_s, c, acc, true, q);
         if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 2)], q);
         if (err == cudaSuccess) err = launch_mlem_normalise_from(n, d_x, c, acc, q);
       } else {
@@ -958,6 +989,302 @@ raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_r
       opts->h_loglik[it] = s1 + ysum * std::log(ysum / s2) - ysum;
     }
   }
+  return RAPTR_OK;
+}
+
+}  // namespace
+
+raptr_status raptr_mlem(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                        const float* d_val, const int64_t* d_col_ptr, const int32_t* d_row_idx, const float* d_tval,
+                        const float* d_y, const float* d_s, float* d_x, int32_t n_iter, const raptr_mlem_opts* opts,
+                        void* stream) {
+  if (!ctx || m < 0 || n <= 0 || n_iter < 0 || !d_row_ptr || !d_y || !d_s || !d_x)
+    return fail(RAPTR_ERR_INVALID, "bad argument");
+  MlemArrays A;
+  A.rp = d_row_ptr;
+  A.col = d_col;
+  A.val = d_val;
+  A.cp = d_col_ptr;
+  A.trow = d_row_idx;
+  A.tval = d_tval;
+  return mlem_impl(ctx, m, n, A, d_y, d_s, d_x, n_iter, opts, as_stream(stream));
+}
+
+raptr_status raptr_mlem_half(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                             const uint16_t* d_hval, const float* d_rscale, const int64_t* d_col_ptr,
+                             const int32_t* d_row_idx, const uint16_t* d_htval, const float* d_y, const float* d_s,
+                             float* d_x, int32_t n_iter, const raptr_mlem_opts* opts, void* stream) {
+  if (!ctx || m < 0 || n <= 0 || n_iter < 0 || !d_row_ptr || !d_y || !d_s || !d_x || !d_col_ptr || !d_htval ||
+      (m > 0 && (!d_hval || !d_rscale)))
+    return fail(RAPTR_ERR_INVALID, "bad argument");
+  MlemArrays A;
+  A.rp = d_row_ptr;
+  A.col = d_col;
+  A.hval = d_hval;
+  A.rscale = d_rscale;
+  A.cp = d_col_ptr;
+  A.trow = d_row_idx;
+  A.htval = d_htval;
+  return mlem_impl(ctx, m, n, A, d_y, d_s, d_x, n_iter, opts, as_stream(stream));
+}
+
+raptr_status raptr_mlem_f64(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
+                            const float* d_val, const int64_t* d_col_ptr, const int32_t* d_row_idx,
+                            const float* d_tval, const int32_t* d_row_rank, const float* d_y, const double* d_s64,
+                            double* d_x64, int32_t n_iter, double* h_loglik, void* stream) {
+  if (!ctx || m < 0 || n <= 0 || n_iter < 0 || !d_row_ptr || !d_col_ptr || !d_y || !d_s64 || !d_x64)
+    return fail(RAPTR_ERR_INVALID, "bad argument");
+  if (n_iter == 0) return RAPTR_OK;
+  DeviceScope ds(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  double *e = nullptr, *xx = nullptr, *acc = nullptr;
+  cudaError_t err = cudaMallocAsync(&e, size_t(std::max<int64_t>(m, 1)) * sizeof(double), s);
+  if (err == cudaSuccess) err = cudaMallocAsync(&xx, size_t(n) * sizeof(double), s);
+  if (err == cudaSuccess) err = cudaMallocAsync(&acc, size_t(2 * n_iter + 2) * sizeof(double), s);
+  if (err == cudaSuccess) err = cudaMemsetAsync(acc, 0, size_t(2 * n_iter + 2) * sizeof(double), s);
+  for (int32_t it = 0; it < n_iter && err == cudaSuccess; it++)
+    err = launch_mlem_f64_iteration(m, n, d_row_ptr, d_col, d_val, d_col_ptr, d_row_idx, d_tval, d_row_rank, d_y,
+                                    d_s64, d_x64, e, xx, acc, h_loglik ? acc + 2 + 2 * it : nullptr, s);
+  std::vector<double> h(size_t(2 * n_iter));
+  double ysum = 0.0;
+  if (err == cudaSuccess && h_loglik) {
+    err = cudaMemcpyAsync(h.data(), acc + 2, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = launch_sum(d_y, m, acc + 1, s);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&ysum, acc + 1, sizeof(double), cudaMemcpyDeviceToHost, s);
+  }
+  if (e) cudaFreeAsync(e, s);
+  if (xx) cudaFreeAsync(xx, s);
+  if (acc) cudaFreeAsync(acc, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return cuda_fail(err, "raptr_mlem_f64");
+  if (h_loglik)
+    for (int32_t it = 0; it < n_iter; it++)
+      h_loglik[it] = h[size_t(2 * it)] + ysum * std::log(ysum / h[size_t(2 * it + 1)]) - ysum;
+  return RAPTR_OK;
+}
+
+raptr_status raptr_matrix_half(raptr_matrix* A, void* stream) {
+  if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
+  if (!A->cp) return fail(RAPTR_ERR_INVALID, "the FP16 form needs the transpose: call raptr_matrix_transpose first");
+  if (A->hval) return RAPTR_OK;
+  DeviceScope ds(A->device);
+  cudaStream_t s = as_stream(stream);
+  const size_t mm = size_t(std::max<int64_t>(A->m, 1)), nz = size_t(std::max<int64_t>(A->nnz, 1));
+  cudaError_t e = cudaMalloc(&A->rscale, mm * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&A->pscale, mm * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&A->hval, nz * sizeof(uint16_t));
+  if (e == cudaSuccess) e = cudaMalloc(&A->htval, nz * sizeof(uint16_t));
+  if (e == cudaSuccess)
+    e = launch_half_convert(A->m, A->nnz, A->rp, A->val, A->trow, A->tval, A->order, A->rscale, A->hval, A->htval,
+                            A->pscale, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    cudaFree(A->rscale);
+    cudaFree(A->pscale);
+    cudaFree(A->hval);
+    cudaFree(A->htval);
+    A->rscale = A->pscale = nullptr;
+    A->hval = A->htval = nullptr;
+    return cuda_fail(e, "raptr_matrix_half");
+  }
+  return RAPTR_OK;
+}
+
+raptr_status raptr_matrix_half_info(const raptr_matrix* A, uint16_t** d_hval, float** d_rscale, uint16_t** d_htval,
+                                    float** d_pscale) {
+  if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
+  if (d_hval) *d_hval = A->hval;
+  if (d_rscale) *d_rscale = A->rscale;
+  if (d_htval) *d_htval = A->htval;
+  if (d_pscale) *d_pscale = A->pscale;
+  return RAPTR_OK;
+}
+
+raptr_status raptr_sensitivity_half(int64_t n, const int64_t* d_col_ptr, const int32_t* d_row_idx,
+                                    const uint16_t* d_htval, const float* d_pscale, double* d_s64, float* d_s32,
+                                    void* stream) {
+  if (n <= 0 || !d_col_ptr || !d_s64) return fail(RAPTR_ERR_INVALID, "bad argument");
+  cudaStream_t s = as_stream(stream);
+  RCU(launch_sens_half(n, d_col_ptr, d_row_idx, d_htval, d_pscale, d_s64, s));
+  if (d_s32) {
+    double* acc = nullptr;
+    RCU(cudaMallocAsync(&acc, sizeof(double), s));
+    cudaError_t e = launch_sum_f64(d_s64, n, acc, s);
+    if (e == cudaSuccess) e = launch_sens_normalise(n, d_s64, acc, d_s32, s);
+    cudaFreeAsync(acc, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sensitivity normalisation");
+  }
+  return RAPTR_OK;
+}
+
+// ---- batched MLEM ----------------------------------------------------------
+
+namespace {
+
+raptr_status batch_args(raptr_ctx* ctx, int64_t m, int64_t n, int32_t K, int32_t value_type, const int64_t* d_row_ptr,
+                        const int32_t* d_col, const void* d_val, const float* d_rscale, const int64_t* d_col_ptr,
+                        const int32_t* d_row_idx, const void* d_tval, const int32_t* d_row_rank, const float* d_y,
+                        const float* d_s, float* d_x, BatchArgs* a) {
+  if (!ctx || m < 0 || n <= 0 || K <= 0 || K > 4096 || (value_type != 0 && value_type != 1) || !d_row_ptr ||
+      !d_col_ptr || !d_y || !d_s || !d_x || (m > 0 && (!d_val || !d_tval)) || (value_type == 1 && m > 0 && !d_rscale))
+    return fail(RAPTR_ERR_INVALID, "bad argument");
+  a->m = m;
+  a->n = n;
+  a->K = K;
+  a->half = value_type == 1;
+  a->rp = d_row_ptr;
+  a->col = d_col;
+  a->val = d_val;
+  a->rscale = d_rscale;
+  a->cp = d_col_ptr;
+  a->trow = d_row_idx;
+  a->tval = d_tval;
+  a->rank = d_row_rank;
+  a->Y = d_y;
+  a->S = d_s;
+  a->X = d_x;
+  return RAPTR_OK;
+}
+
+int default_frame_tile(int K) {
+  for (int kt : {32, 16, 8, 4, 64})
+    if (batch_tile_supported(K, kt)) return kt;
+  return 0;
+}
+
+}  // namespace
+
+raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_frames, int32_t value_type,
+                              const int64_t* d_row_ptr, const int32_t* d_col, const void* d_val,
+                              const float* d_rscale, const int64_t* d_col_ptr, const int32_t* d_row_idx,
+                              const void* d_tval, const int32_t* d_row_rank, const float* d_y, const float* d_s,
+                              float* d_x, int32_t n_iter, int32_t frame_tile, const raptr_mlem_opts* opts,
+                              void* stream) {
+  BatchArgs a;
+  RCHECK(batch_args(ctx, m, n, n_frames, value_type, d_row_ptr, d_col, d_val, d_rscale, d_col_ptr, d_row_idx, d_tval,
+                    d_row_rank, d_y, d_s, d_x, &a));
+  if (n_iter < 0) return fail(RAPTR_ERR_INVALID, "bad argument");
+  const int kt = frame_tile > 0 ? frame_tile : default_frame_tile(n_frames);
+  if (!batch_tile_supported(n_frames, kt))
+    return fail(RAPTR_ERR_INVALID, "frame tile must be 4, 8, 16, 32 or 64 and divide the number of frames");
+  if (n_iter == 0) return RAPTR_OK;
+  DeviceScope ds(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  const bool want_times = opts && opts->h_kernel_ms;
+  const bool use_graph = opts && opts->use_graph && !want_times;
+  RCHECK(ctx->ensure_scratch(Carve::need({size_t(std::max<int64_t>(m, 1)) * n_frames * sizeof(float),
+                                          size_t(n) * n_frames * sizeof(float), size_t(n_frames) * sizeof(double)})));
+  Carve cv(ctx->d_scratch);
+  a.E = cv.take<float>(size_t(std::max<int64_t>(m, 1)) * n_frames);
+  a.XX = cv.take<float>(size_t(n) * n_frames);
+  double* acc = cv.take<double>(size_t(n_frames));
+  std::vector<cudaEvent_t> evs;
+  if (want_times) {
+    evs.resize(size_t(3 * n_iter));
+    for (auto& ev : evs) RCU(cudaEventCreate(&ev));
+  }
+  auto enqueue = [&](cudaStream_t q) -> cudaError_t {
+    for (int32_t it = 0; it < n_iter; it++) {
+      cudaError_t err = cudaSuccess;
+      if (want_times) err = cudaEventRecord(evs[size_t(3 * it)], q);
+      if (err == cudaSuccess) err = launch_batch_iteration(a, kt, acc, q, want_times ? evs[size_t(3 * it + 1)] : nullptr);
+      if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 2)], q);
+      if (err != cudaSuccess) return err;
+    }
+    return cudaSuccess;
+  };
+  if (!use_graph) {
+    RCU(enqueue(s));
+  } else {
+    cudaStream_t cap;
+    RCU(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaEvent_t ev;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cap, ev, 0);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const long long before = launches_so_far();
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      cudaError_t e1 = enqueue(cap);
+      cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+      e = (e1 != cudaSuccess) ? e1 : e2;
+    }
+    const long long captured = launches_so_far() - before;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, cap);
+    if (e == cudaSuccess) note_launches(captured);  // the replay launches them again
+    if (e == cudaSuccess) e = cudaEventRecord(ev, cap);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cap);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaEventDestroy(ev);
+    cudaStreamDestroy(cap);
+    if (e != cudaSuccess) return cuda_fail(e, "batched MLEM graph");
+  }
+  if (want_times) {
+    RCU(cudaStreamSynchronize(s));
+    for (int32_t it = 0; it < n_iter; it++) {
+      float t0 = 0.f, t1 = 0.f;
+      RCU(cudaEventElapsedTime(&t0, evs[size_t(3 * it)], evs[size_t(3 * it + 1)]));
+      RCU(cudaEventElapsedTime(&t1, evs[size_t(3 * it + 1)], evs[size_t(3 * it + 2)]));
+      opts->h_kernel_ms[2 * it] = t0;
+      opts->h_kernel_ms[2 * it + 1] = t1;
+    }
+    for (auto& ev : evs) cudaEventDestroy(ev);
+  }
+  return RAPTR_OK;
+}
+
+raptr_status raptr_mlem_batch_autotune(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_frames, int32_t value_type,
+                                       const int64_t* d_row_ptr, const int32_t* d_col, const void* d_val,
+                                       const float* d_rscale, const int64_t* d_col_ptr, const int32_t* d_row_idx,
+                                       const void* d_tval, const int32_t* d_row_rank, const float* d_y,
+                                       const float* d_s, const float* d_x, int32_t* best_tile, float* h_ms,
+                                       void* stream) {
+  if (!best_tile) return fail(RAPTR_ERR_INVALID, "bad argument");
+  DeviceScope ds(ctx ? ctx->device : 0);
+  cudaStream_t s = as_stream(stream);
+  // time one iteration per candidate tile on a copy of the images
+  float* xc = nullptr;
+  RCU(cudaMallocAsync(&xc, size_t(n) * n_frames * sizeof(float), s));
+  const int tiles[5] = {4, 8, 16, 32, 64};
+  float best = 0.f;
+  *best_tile = 0;
+  raptr_status st = RAPTR_OK;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int i = 0; i < 5 && st == RAPTR_OK; i++) {
+    const int kt = tiles[i];
+    if (h_ms) h_ms[i] = -1.f;
+    if (!batch_tile_supported(n_frames, kt)) continue;
+    float ms = 0.f;
+    for (int rep = 0; rep < 3 && st == RAPTR_OK; rep++) {  // first is a warm-up
+      cudaMemcpyAsync(xc, d_x, size_t(n) * n_frames * sizeof(float), cudaMemcpyDeviceToDevice, s);
+      cudaEventRecord(e0, s);
+      st = raptr_mlem_batch(ctx, m, n, n_frames, value_type, d_row_ptr, d_col, d_val, d_rscale, d_col_ptr, d_row_idx,
+                            d_tval, d_row_rank, d_y, d_s, xc, 1, kt, nullptr, stream);
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep > 0) ms += t / 2;
+    }
+    if (h_ms) h_ms[i] = ms;
+    if (st == RAPTR_OK && (*best_tile == 0 || ms < best)) {
+      best = ms;
+      *best_tile = kt;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(xc, s);
+  cudaStreamSynchronize(s);
+  if (st != RAPTR_OK) return st;
+  if (*best_tile == 0) return fail(RAPTR_ERR_INVALID, "no frame tile divides the number of frames");
   return RAPTR_OK;
 }
 

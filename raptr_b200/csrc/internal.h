@@ -102,6 +102,59 @@ cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s);
 
 // Transpose (CSC) of a CSR matrix: column counts (int32 atomics), widening to
 // int64, and the fill through per-column cursors (initialised to col_ptr).
+// ---- precision forms (kernels_precision.cu) --------------------------------
+
+// FP16 copy of a matrix: rscale (m), hval (nnz, CSR order), htval (nnz,
+// order of the transpose trow/tval, whose index is a position in `order`
+// or the row when order is null), pscale (m, rscale by position).
+cudaError_t launch_half_convert(int64_t m, int64_t nnz, const int64_t* rp, const float* val, const int32_t* trow,
+                                const float* tval, const int32_t* order, float* rscale, uint16_t* hval,
+                                uint16_t* htval, float* pscale, cudaStream_t s);
+// FP64 column sums of the FP16 matrix through its transpose.
+cudaError_t launch_sens_half(int64_t n, const int64_t* cp, const int32_t* trow, const uint16_t* htval,
+                             const float* pscale, double* s64, cudaStream_t s);
+// e[rank_i] = rscale_i * y_i / (A x)_i (0 where y_i == 0).
+cudaError_t launch_mlem_forward_half(int64_t m, const int64_t* rp, const int32_t* col, const uint16_t* hval,
+                                     const float* rscale, const float* y, const float* x, const int32_t* rank,
+                                     float* e, double* d_ll, cudaStream_t s);
+// c_j = sum h_kj e_k, compensated; with update as launch_mlem_back.
+cudaError_t launch_mlem_back_half(int64_t n, const int64_t* cp, const int32_t* trow, const uint16_t* htval,
+                                  const float* e, const float* x, const float* sens, float* out, double* d_acc,
+                                  bool update, cudaStream_t s);
+// One MLEM iteration with FP64 vectors (x, e, xx: n / m / n doubles, acc one
+// double); s64 is the normalised sensitivity.
+cudaError_t launch_mlem_f64_iteration(int64_t m, int64_t n, const int64_t* rp, const int32_t* col, const float* val,
+                                      const int64_t* cp, const int32_t* trow, const float* tval, const int32_t* rank,
+                                      const float* y, const double* s64, double* x, double* e, double* xx,
+                                      double* acc, double* d_ll, cudaStream_t s);
+
+// ---- batched MLEM (kernels_batch.cu) ---------------------------------------
+
+// K frames over one matrix (FP16 values with row scales when half, else
+// FP32); X, Y frame-minor (n x K, m x K); E (m x K) and XX (n x K) scratch.
+struct BatchArgs {
+  int64_t m = 0, n = 0;
+  int K = 0;
+  bool half = false;
+  const int64_t* rp = nullptr;
+  const int32_t* col = nullptr;
+  const void* val = nullptr;
+  const float* rscale = nullptr;
+  const int64_t* cp = nullptr;
+  const int32_t* trow = nullptr;
+  const void* tval = nullptr;
+  const int32_t* rank = nullptr;
+  const float* Y = nullptr;
+  const float* S = nullptr;
+  float* X = nullptr;
+  float* E = nullptr;
+  float* XX = nullptr;
+};
+bool batch_tile_supported(int K, int kt);
+// One iteration for all K frames in tiles of kt frames (acc: K doubles of
+// scratch); ev_mid, when set, is recorded between the two passes.
+cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, cudaStream_t s, cudaEvent_t ev_mid);
+
 // Back-projection order of a list of channels (kernels_util.cu): key per
 // channel in [0, channel_order_keys(g)); mark counts keys (bad |= 1 on a
 // repeated key or a channel out of range); with prefix = exclusive scan of
