@@ -312,7 +312,8 @@ raptr_status raptr_mlem_f64(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t*
  * htval, d_rscale the row scales); the transpose is required and d_row_rank
  * follows it (raptr_matrix_row_order, may be null for the natural order).
  * Each pass handles frame_tile frames per sweep of the matrix (4, 8, 16, 32
- * or 64, dividing n_frames; 0 = the default 32-or-smaller divisor).
+ * or 64, dividing n_frames; 0 = the default 32-or-smaller divisor); d_x
+ * must be 16-byte aligned.
  * opts: use_graph captures the n_iter iterations in a CUDA graph;
  * h_kernel_ms receives per iteration the forward and back-pass times. */
 raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_frames, int32_t value_type,

@@ -115,6 +115,34 @@ struct raptr_ctx {
   int64_t* d_i64 = nullptr;   // 64 entries
   int32_t* d_flags = nullptr; // 16 entries
   double* d_f64 = nullptr;    // 64 entries
+  // Voxels in compact (y, z) tubes along x: the column order of the
+  // batched back pass, built on first use.
+  int32_t* d_col_order = nullptr;
+
+  cudaError_t col_order(const int32_t** out) {
+    if (!d_col_order) {
+      const int nx = dg.n[0], ny = dg.n[1], nz = dg.n[2];
+      // about one wave of warps (148 SMs x 64) per tube
+      int tb = int(std::lround(std::sqrt(9472.0 / std::max(nx, 1))));
+      tb = std::max(1, std::min(tb, std::max(ny, nz)));
+      std::vector<int32_t> h;
+      h.reserve(size_t(nx) * ny * nz);
+      for (int ty = 0; ty < ny; ty += tb)
+        for (int tz = 0; tz < nz; tz += tb)
+          for (int x = 0; x < nx; x++)
+            for (int y = ty; y < std::min(ny, ty + tb); y++)
+              for (int z = tz; z < std::min(nz, tz + tb); z++) h.push_back(int32_t((int64_t(x) * ny + y) * nz + z));
+      cudaError_t e = cudaMalloc(&d_col_order, h.size() * sizeof(int32_t));
+      if (e == cudaSuccess) e = cudaMemcpy(d_col_order, h.data(), h.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        cudaFree(d_col_order);
+        d_col_order = nullptr;
+        return e;
+      }
+    }
+    *out = d_col_order;
+    return cudaSuccess;
+  }
 
   raptr_status ensure_scratch(size_t bytes) {
     if (bytes <= scratch_bytes) return RAPTR_OK;
@@ -350,6 +378,7 @@ raptr_status raptr_ctx_destroy(raptr_ctx* ctx) {
   cudaFree(ctx->d_i64);
   cudaFree(ctx->d_flags);
   cudaFree(ctx->d_f64);
+  cudaFree(ctx->d_col_order);
   delete ctx;
   return RAPTR_OK;
 }
@@ -1128,6 +1157,9 @@ raptr_status batch_args(raptr_ctx* ctx, int64_t m, int64_t n, int32_t K, int32_t
   if (!ctx || m < 0 || n <= 0 || K <= 0 || K > 4096 || (value_type != 0 && value_type != 1) || !d_row_ptr ||
       !d_col_ptr || !d_y || !d_s || !d_x || (m > 0 && (!d_val || !d_tval)) || (value_type == 1 && m > 0 && !d_rscale))
     return fail(RAPTR_ERR_INVALID, "bad argument");
+  // the passes gather four frames at a time (16-byte loads of the images)
+  if ((reinterpret_cast<uintptr_t>(d_x) & 15u) != 0)
+    return fail(RAPTR_ERR_INVALID, "the images must be 16-byte aligned");
   a->m = m;
   a->n = n;
   a->K = K;
@@ -1173,11 +1205,16 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
   const bool want_times = opts && opts->h_kernel_ms;
   const bool use_graph = opts && opts->use_graph && !want_times;
   RCHECK(ctx->ensure_scratch(Carve::need({size_t(std::max<int64_t>(m, 1)) * n_frames * sizeof(float),
-                                          size_t(n) * n_frames * sizeof(float), size_t(n_frames) * sizeof(double)})));
+                                          size_t(n) * n_frames * sizeof(float), size_t(n_frames) * sizeof(double),
+                                          size_t(n_frames) * sizeof(unsigned long long)})));
   Carve cv(ctx->d_scratch);
+  // the tube order of the back pass applies when the columns are the
+  // context's voxels
+  if (n == int64_t(ctx->dg.n[0]) * ctx->dg.n[1] * ctx->dg.n[2]) RCU(ctx->col_order(&a.col_order));
   a.E = cv.take<float>(size_t(std::max<int64_t>(m, 1)) * n_frames);
   a.XX = cv.take<float>(size_t(n) * n_frames);
   double* acc = cv.take<double>(size_t(n_frames));
+  unsigned long long* next = cv.take<unsigned long long>(size_t(n_frames));
   std::vector<cudaEvent_t> evs;
   if (want_times) {
     evs.resize(size_t(3 * n_iter));
@@ -1187,7 +1224,7 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
     for (int32_t it = 0; it < n_iter; it++) {
       cudaError_t err = cudaSuccess;
       if (want_times) err = cudaEventRecord(evs[size_t(3 * it)], q);
-      if (err == cudaSuccess) err = launch_batch_iteration(a, kt, acc, q, want_times ? evs[size_t(3 * it + 1)] : nullptr);
+      if (err == cudaSuccess) err = launch_batch_iteration(a, kt, acc, next, q, want_times ? evs[size_t(3 * it + 1)] : nullptr);
       if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 2)], q);
       if (err != cudaSuccess) return err;
     }

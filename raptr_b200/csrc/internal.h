@@ -144,6 +144,7 @@ struct BatchArgs {
   const int32_t* trow = nullptr;
   const void* tval = nullptr;
   const int32_t* rank = nullptr;
+  const int32_t* col_order = nullptr;  // back-pass column order (may be null)
   const float* Y = nullptr;
   const float* S = nullptr;
   float* X = nullptr;
@@ -151,9 +152,11 @@ struct BatchArgs {
   float* XX = nullptr;
 };
 bool batch_tile_supported(int K, int kt);
-// One iteration for all K frames in tiles of kt frames (acc: K doubles of
-// scratch); ev_mid, when set, is recorded between the two passes.
-cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, cudaStream_t s, cudaEvent_t ev_mid);
+// One iteration for all K frames in tiles of kt frames (acc: K doubles,
+// next: K/kt work counters, both scratch); ev_mid, when set, is recorded
+// between the two passes.
+cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, unsigned long long* next, cudaStream_t s,
+                                   cudaEvent_t ev_mid);
 
 // Back-projection order of a list of channels (kernels_util.cu): key per
 // channel in [0, channel_order_keys(g)); mark counts keys (bad |= 1 on a

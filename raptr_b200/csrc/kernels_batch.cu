@@ -10,7 +10,10 @@
 // step a warp reads EPW matrix entries and gathers EPW rows of KT frames,
 // coalesced.  The value type is binary16 (with the per-row scale folded
 // into E, as in the FP16 single-frame form) or float.  Grids are sized to
-// the GPU and every warp loops over rows / columns (persistent CTAs).
+// the GPU and every warp loops over rows / columns (persistent CTAs).  The
+// back pass can take the columns in a given order: voxels in compact
+// (y, z) tubes along x keep the ratio rows that concurrent warps gather
+// (the channels crossing those voxels) within L2.
 #include <cstdint>
 
 #include <cuda_fp16.h>
@@ -33,20 +36,21 @@ unsigned grid_warps(int64_t items) {
 __device__ __forceinline__ float to_f(float v) { return v; }
 __device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
 
+// Four frames per lane (one 16-byte gather), KT/4 lanes per entry slot.
 template <int KT>
 struct Split {
-  static constexpr int VEC = KT >= 32 ? KT / 32 : 1;
+  static constexpr int VEC = 4;
   static constexpr int LPE = KT / VEC;
   static constexpr int EPW = 32 / LPE;
 };
 
-__device__ __forceinline__ void two_sum_add(float& s, float& c, float v) {
-  const float t = s + v;
-  if (fabsf(s) >= fabsf(v))
-    c += (s - t) + v;
-  else
-    c += (v - t) + s;
-  s = t;
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+__device__ __forceinline__ void fma4(float (&a)[4], float w, float4 x) {
+  a[0] += w * x.x;
+  a[1] += w * x.y;
+  a[2] += w * x.z;
+  a[3] += w * x.w;
 }
 
 // Forward: E[rank_i*K + f] = sc_i * Y[i*K + f] / (sc_i * sum_j v_ij X[j*K + f])
@@ -76,18 +80,12 @@ __global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int 
     for (; k + S::EPW < e; k += 2 * S::EPW) {
       const int c0 = __ldg(col + k), c1 = __ldg(col + k + S::EPW);
       const float w0 = to_f(val[k]), w1 = to_f(val[k + S::EPW]);
-      const float* x0 = X + int64_t(c0) * K + fbase;
-      const float* x1 = X + int64_t(c1) * K + fbase;
-#pragma unroll
-      for (int v = 0; v < S::VEC; v++) acc[v] += w0 * __ldg(x0 + v) + w1 * __ldg(x1 + v);
+      const float4 x0 = ld4(X + int64_t(c0) * K + fbase);
+      const float4 x1 = ld4(X + int64_t(c1) * K + fbase);
+      fma4(acc, w0, x0);
+      fma4(acc, w1, x1);
     }
-    if (k < e) {
-      const int c0 = __ldg(col + k);
-      const float w0 = to_f(val[k]);
-      const float* x0 = X + int64_t(c0) * K + fbase;
-#pragma unroll
-      for (int v = 0; v < S::VEC; v++) acc[v] += w0 * __ldg(x0 + v);
-    }
+    if (k < e) fma4(acc, to_f(val[k]), ld4(X + int64_t(__ldg(col + k)) * K + fbase));
 #pragma unroll
     for (int o = S::LPE; o < 32; o <<= 1)
 #pragma unroll
@@ -105,16 +103,18 @@ __global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int 
 }
 
 // Back projection and update for the frames of the tile:
-// c = sum_k v_kj E[k*K + f] (compensated), XX = X*c/(S+(S==0)),
-// acc[f] += sum_j XX (FP64).
+// c = sum_k v_kj E[k*K + f] (FP32; the FP16 values dominate its error),
+// XX = X*c/(S+(S==0)), acc[f] += sum_j XX (FP64).  Warps take columns from
+// the counter *next (zero at launch).
 template <int KT, typename VT>
-__global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, int f0,
+__global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, int f0, unsigned long long* next,
                                                               const int64_t* __restrict__ cp,
                                                               const int32_t* __restrict__ trow,
                                                               const VT* __restrict__ tval,
                                                               const float* __restrict__ E,
                                                               const float* __restrict__ X,
                                                               const float* __restrict__ sens,
+                                                              const int32_t* __restrict__ col_order,
                                                               float* __restrict__ XX, double* __restrict__ acc) {
   using S = Split<KT>;
   const int lane = threadIdx.x & 31;
@@ -124,42 +124,38 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
   double fsum[S::VEC];
 #pragma unroll
   for (int v = 0; v < S::VEC; v++) fsum[v] = 0.0;
-  for (int64_t j = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; j < n; j += nw) {
-    float s[S::VEC], c[S::VEC];
+  (void)nw;
+  for (;;) {
+    // columns are handed out one at a time (their lengths vary ~20-fold)
+    unsigned long long q = 0;
+    if (lane == 0) q = atomicAdd(next, 1ull);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= (unsigned long long)n) break;
+    const int64_t j = col_order ? int64_t(__ldg(col_order + q)) : int64_t(q);
+    float s[S::VEC];
 #pragma unroll
-    for (int v = 0; v < S::VEC; v++) s[v] = c[v] = 0.f;
+    for (int v = 0; v < S::VEC; v++) s[v] = 0.f;
     const int64_t b = cp[j], e = cp[j + 1];
     int64_t p = b + es;
     for (; p + S::EPW < e; p += 2 * S::EPW) {
       const int k0 = __ldg(trow + p), k1 = __ldg(trow + p + S::EPW);
       const float w0 = to_f(tval[p]), w1 = to_f(tval[p + S::EPW]);
-      const float* e0 = E + int64_t(k0) * K + fbase;
-      const float* e1 = E + int64_t(k1) * K + fbase;
-#pragma unroll
-      for (int v = 0; v < S::VEC; v++) two_sum_add(s[v], c[v], w0 * __ldg(e0 + v) + w1 * __ldg(e1 + v));
+      const float4 e0 = ld4(E + int64_t(k0) * K + fbase);
+      const float4 e1 = ld4(E + int64_t(k1) * K + fbase);
+      fma4(s, w0, e0);
+      fma4(s, w1, e1);
     }
-    if (p < e) {
-      const int k0 = __ldg(trow + p);
-      const float w0 = to_f(tval[p]);
-      const float* e0 = E + int64_t(k0) * K + fbase;
-#pragma unroll
-      for (int v = 0; v < S::VEC; v++) two_sum_add(s[v], c[v], w0 * __ldg(e0 + v));
-    }
+    if (p < e) fma4(s, to_f(tval[p]), ld4(E + int64_t(__ldg(trow + p)) * K + fbase));
 #pragma unroll
     for (int o = S::LPE; o < 32; o <<= 1)
 #pragma unroll
-      for (int v = 0; v < S::VEC; v++) {
-        const float so = __shfl_xor_sync(0xffffffffu, s[v], o);
-        const float co = __shfl_xor_sync(0xffffffffu, c[v], o);
-        two_sum_add(s[v], c[v], so);
-        c[v] += co;
-      }
+      for (int v = 0; v < S::VEC; v++) s[v] += __shfl_xor_sync(0xffffffffu, s[v], o);
     if (es == 0) {
       float dvs = __ldg(sens + j);
       dvs += float(dvs == 0.f);
 #pragma unroll
       for (int v = 0; v < S::VEC; v++) {
-        const float xx = __fdiv_rn(__fmul_rn(X[j * K + fbase + v], s[v] + c[v]), dvs);
+        const float xx = __fdiv_rn(__fmul_rn(X[j * K + fbase + v], s[v]), dvs);
         XX[j * K + fbase + v] = xx;
         fsum[v] += double(xx);
       }
@@ -184,14 +180,15 @@ __global__ void batch_normalise_kernel(int64_t n, int K, float* __restrict__ X, 
 template <int KT, typename VT>
 cudaError_t launch_tile(bool forward, int64_t m, int64_t n, int K, int f0, const int64_t* rp, const int32_t* col,
                         const void* val, const float* rscale, const int64_t* cp, const int32_t* trow,
-                        const void* tval, const int32_t* rank, const float* Y, const float* S, float* X, float* E,
-                        float* XX, double* acc, cudaStream_t s) {
+                        const void* tval, const int32_t* rank, const int32_t* col_order, const float* Y,
+                        const float* S, float* X, float* E, float* XX, double* acc, unsigned long long* next,
+                        cudaStream_t s) {
   if (forward)
     batch_forward_kernel<KT, VT><<<grid_warps(m), kThreads, 0, s>>>(m, K, f0, rp, col, static_cast<const VT*>(val),
                                                                     rscale, Y, X, rank, E);
   else
-    batch_back_kernel<KT, VT><<<grid_warps(n), kThreads, 0, s>>>(n, K, f0, cp, trow, static_cast<const VT*>(tval),
-                                                                 E, X, S, XX, acc);
+    batch_back_kernel<KT, VT><<<grid_warps(n), kThreads, 0, s>>>(n, K, f0, next, cp, trow, static_cast<const VT*>(tval),
+                                                                 E, X, S, col_order, XX, acc);
   note_launches(1);
   return cudaGetLastError();
 }
@@ -199,22 +196,23 @@ cudaError_t launch_tile(bool forward, int64_t m, int64_t n, int K, int f0, const
 template <typename VT>
 cudaError_t launch_tile_kt(int kt, bool forward, int64_t m, int64_t n, int K, int f0, const int64_t* rp,
                            const int32_t* col, const void* val, const float* rscale, const int64_t* cp,
-                           const int32_t* trow, const void* tval, const int32_t* rank, const float* Y,
-                           const float* S, float* X, float* E, float* XX, double* acc, cudaStream_t s) {
+                           const int32_t* trow, const void* tval, const int32_t* rank, const int32_t* col_order,
+                           const float* Y, const float* S, float* X, float* E, float* XX, double* acc,
+                           unsigned long long* next, cudaStream_t s) {
   switch (kt) {
     case 4:
-      return launch_tile<4, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, Y, S, X, E, XX, acc, s);
+      return launch_tile<4, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E, XX, acc, next, s);
     case 8:
-      return launch_tile<8, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, Y, S, X, E, XX, acc, s);
+      return launch_tile<8, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E, XX, acc, next, s);
     case 16:
-      return launch_tile<16, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, Y, S, X, E, XX, acc,
-                                 s);
+      return launch_tile<16, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E,
+                                 XX, acc, next, s);
     case 32:
-      return launch_tile<32, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, Y, S, X, E, XX, acc,
-                                 s);
+      return launch_tile<32, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E,
+                                 XX, acc, next, s);
     case 64:
-      return launch_tile<64, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, Y, S, X, E, XX, acc,
-                                 s);
+      return launch_tile<64, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E,
+                                 XX, acc, next, s);
     default:
       return cudaErrorInvalidValue;
   }
@@ -226,19 +224,22 @@ bool batch_tile_supported(int K, int kt) {
   return (kt == 4 || kt == 8 || kt == 16 || kt == 32 || kt == 64) && K > 0 && K % kt == 0;
 }
 
-cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, cudaStream_t s, cudaEvent_t ev_mid) {
+cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, unsigned long long* next, cudaStream_t s,
+                                   cudaEvent_t ev_mid) {
   cudaError_t e = cudaMemsetAsync(acc, 0, size_t(a.K) * sizeof(double), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(next, 0, size_t(a.K / kt) * sizeof(unsigned long long), s);
   for (int f0 = 0; f0 < a.K && e == cudaSuccess; f0 += kt)
     e = a.half ? launch_tile_kt<__half>(kt, true, a.m, a.n, a.K, f0, a.rp, a.col, a.val, a.rscale, a.cp, a.trow,
-                                        a.tval, a.rank, a.Y, a.S, a.X, a.E, a.XX, acc, s)
+                                        a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, nullptr, s)
                : launch_tile_kt<float>(kt, true, a.m, a.n, a.K, f0, a.rp, a.col, a.val, nullptr, a.cp, a.trow,
-                                       a.tval, a.rank, a.Y, a.S, a.X, a.E, a.XX, acc, s);
+                                       a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, nullptr, s);
   if (e == cudaSuccess && ev_mid) e = cudaEventRecord(ev_mid, s);
   for (int f0 = 0; f0 < a.K && e == cudaSuccess; f0 += kt)
     e = a.half ? launch_tile_kt<__half>(kt, false, a.m, a.n, a.K, f0, a.rp, a.col, a.val, a.rscale, a.cp, a.trow,
-                                        a.tval, a.rank, a.Y, a.S, a.X, a.E, a.XX, acc, s)
+                                        a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, next + f0 / kt,
+                                        s)
                : launch_tile_kt<float>(kt, false, a.m, a.n, a.K, f0, a.rp, a.col, a.val, nullptr, a.cp, a.trow,
-                                       a.tval, a.rank, a.Y, a.S, a.X, a.E, a.XX, acc, s);
+                                       a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, next + f0 / kt, s);
   if (e == cudaSuccess) {
     const int64_t total = a.n * a.K;
     int64_t blocks = (total + kThreads - 1) / kThreads;
