@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) mlem_forward_half_kernel(
 
 // Column dot with binary16 values and compensated accumulation; lane q
 // takes quads q, q+32, ... (four consecutive entries: 16-byte index load,
-// 8-byte value load).
+// 8-byte value load), each quad summed in FP32 and added with a two-sum.
 __device__ __forceinline__ float col_dot_half(const int32_t* __restrict__ trow, const uint16_t* __restrict__ hv,
                                               int64_t b, int64_t e, const float* __restrict__ ev, int lane) {
   float s = 0.f, c = 0.f;
@@ -196,18 +196,16 @@ __device__ __forceinline__ float col_dot_half(const int32_t* __restrict__ trow, 
     const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&w0.y));
     const float2 f2 = __half22float2(*reinterpret_cast<const __half2*>(&w1.x));
     const float2 f3 = __half22float2(*reinterpret_cast<const __half2*>(&w1.y));
-    two_sum_add(s, c, f0.x * g0 + f0.y * g1);
-    two_sum_add(s, c, f1.x * g2 + f1.y * g3);
-    two_sum_add(s, c, f2.x * g4 + f2.y * g5);
-    two_sum_add(s, c, f3.x * g6 + f3.y * g7);
+    two_sum_add(s, c, (f0.x * g0 + f0.y * g1) + (f1.x * g2 + f1.y * g3));
+    two_sum_add(s, c, (f2.x * g4 + f2.y * g5) + (f3.x * g6 + f3.y * g7));
   }
   for (; q < nq; q += 32) {
     const int4 r0 = __ldcs(t4 + q);
     const uint2 w0 = __ldcs(h4 + q);
     const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&w0.x));
     const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&w0.y));
-    two_sum_add(s, c, f0.x * __ldg(ev + r0.x) + f0.y * __ldg(ev + r0.y));
-    two_sum_add(s, c, f1.x * __ldg(ev + r0.z) + f1.y * __ldg(ev + r0.w));
+    two_sum_add(s, c, (f0.x * __ldg(ev + r0.x) + f0.y * __ldg(ev + r0.y)) +
+                          (f1.x * __ldg(ev + r0.z) + f1.y * __ldg(ev + r0.w)));
   }
   const int64_t t = a + (nq << 2) + lane;
   if (t < e) two_sum_add(s, c, h2f(hv[t]) * __ldg(ev + __ldg(trow + t)));
