@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define RAPTR_ABI_VERSION 2
+#define RAPTR_ABI_VERSION 3
 
 typedef enum raptr_status {
   RAPTR_OK = 0,
@@ -44,7 +44,8 @@ typedef enum raptr_status {
   RAPTR_ERR_CAPACITY = 3,    /* caller buffer too small; required size returned     */
   RAPTR_ERR_OVERFLOW = 4,    /* an internal per-row table overflowed (after retry)  */
   RAPTR_ERR_NOMEM = 5,       /* device allocation failed                            */
-  RAPTR_ERR_UNSUPPORTED = 6  /* feature not available for these arguments           */
+  RAPTR_ERR_UNSUPPORTED = 6, /* feature not available for these arguments           */
+  RAPTR_ERR_TIMEOUT = 7      /* a wait ended before the work finished               */
 } raptr_status;
 
 /* Scanner geometry.  Field meaning and units as in DefaultVoxelGrid
@@ -281,6 +282,12 @@ raptr_status raptr_mlem_forward_ordered(int64_t m, const int64_t* d_row_ptr, con
 raptr_status raptr_matrix_half(raptr_matrix* A, void* stream);
 raptr_status raptr_matrix_half_info(const raptr_matrix* A, uint16_t** d_hval, float** d_rscale, uint16_t** d_htval,
                                     float** d_pscale);
+/* Frees the FP32 values of the CSR and its transpose once the FP16 form
+ * exists (the FP16 iterations need only indices and binary16 values);
+ * raptr_matrix_info / raptr_matrix_csc_info then return null values. */
+raptr_status raptr_matrix_drop_f32(raptr_matrix* A);
+/* Device bytes held by the matrix (all its forms). */
+raptr_status raptr_matrix_bytes(const raptr_matrix* A, int64_t* bytes);
 /* FP64 column sums of the FP16 matrix (through its transpose), and the same
  * normalised to sum 1 in float when d_s32 is non-null. */
 raptr_status raptr_sensitivity_half(int64_t n, const int64_t* d_col_ptr, const int32_t* d_row_idx,
@@ -349,6 +356,54 @@ raptr_status raptr_mlem_batch_autotune(raptr_ctx* ctx, int64_t m, int64_t n, int
 raptr_status raptr_mlem_noalloc(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
                                 const float* d_val, const float* d_y, const float* d_s, float* d_x, int32_t n_iter,
                                 void* stream);
+
+/* ---- serving ----------------------------------------------------------------
+ * No counterpart in the reference (one reconstruction per process run).
+ * A server runs MLEM reconstructions of mixed geometry on one GPU as they
+ * are submitted: a worker thread keeps one system matrix per (geometry,
+ * rays, seed) resident -- FP16 form with its transpose, built on the first
+ * request, evicted least recently used when the HBM budget needs room --
+ * and iterates all admitted requests of a geometry together (batched
+ * frames, one CUDA stream per geometry so that geometries overlap on the
+ * device).  Requests join and leave between iterations; each keeps its own
+ * iteration count.  A request waits in the queue while its matrix and
+ * state do not fit the budget (and fails with RAPTR_ERR_NOMEM when they
+ * never can).  Each result equals the batched FP16 iteration of that
+ * request alone, up to summation order. */
+typedef struct raptr_server raptr_server;
+typedef struct raptr_server_opts {
+  int64_t hbm_budget_bytes; /* resident matrices + request state; leave room for
+                               a build's transient memory (~24 bytes/entry)   */
+  int32_t max_frames;       /* requests per geometry batch, 1..64              */
+  int32_t keep_fp32;        /* keep the FP32 values of cached matrices         */
+} raptr_server_opts;
+typedef struct raptr_request_stats {
+  double queue_ms;   /* submit -> admitted                                    */
+  double run_ms;     /* admitted -> result on the host                        */
+  double total_ms;   /* submit -> result on the host                          */
+  int32_t iterations;
+  int32_t frames_max; /* largest batch the request ran in                     */
+  int32_t cold_build; /* 1 when its admission built the matrix                */
+} raptr_request_stats;
+typedef struct raptr_server_stats {
+  int64_t submitted, completed, iterations, batch_steps, builds, evictions;
+  int64_t resident_matrices, resident_bytes, queued, running;
+} raptr_server_stats;
+raptr_status raptr_server_create(int32_t device, const raptr_server_opts* opts, raptr_server** out);
+/* Stops the worker (running and queued requests fail) and frees the device
+ * memory. */
+raptr_status raptr_server_destroy(raptr_server* s);
+/* Queues a reconstruction: h_y holds the counts of all channels of the
+ * geometry (channel id order, copied), n_iter MLEM iterations from a
+ * uniform image. */
+raptr_status raptr_server_submit(raptr_server* s, const raptr_geom* geom, int32_t nrays, uint32_t seed,
+                                 const float* h_y, int32_t n_iter, int64_t* request_id);
+/* Waits (timeout_ms < 0: without limit) for a request, copies its image
+ * (voxels of the geometry) to h_x when non-null and forgets the request.
+ * RAPTR_ERR_TIMEOUT leaves it pending. */
+raptr_status raptr_server_wait(raptr_server* s, int64_t request_id, float* h_x, int32_t timeout_ms,
+                               raptr_request_stats* stats);
+raptr_status raptr_server_get_stats(raptr_server* s, raptr_server_stats* out);
 
 /* ---- end-to-end ------------------------------------------------------------ */
 

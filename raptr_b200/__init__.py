@@ -58,6 +58,20 @@ class raptr_mlem_opts(C.Structure):
                 ("d_row_rank", C.c_void_p)]
 
 
+class raptr_server_opts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_frames", C.c_int32), ("keep_fp32", C.c_int32)]
+
+
+class raptr_request_stats(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("run_ms", C.c_double), ("total_ms", C.c_double),
+                ("iterations", C.c_int32), ("frames_max", C.c_int32), ("cold_build", C.c_int32)]
+
+
+class raptr_server_stats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "completed", "iterations", "batch_steps", "builds", "evictions",
+                                         "resident_matrices", "resident_bytes", "queued", "running")]
+
+
 class raptr_reco_stats(C.Structure):
     _fields_ = [
         ("build_ms", C.c_double),
@@ -138,6 +152,13 @@ _SIGNATURES = {
     "raptr_row_ptr_widen": (C.c_int, [VP, I64, VP, VP]),
     "raptr_reco_host": (C.c_int, [C.POINTER(raptr_geom), C.c_int, VP, I32, C.c_uint32, I32, VP, VP, VP,
                                   C.POINTER(raptr_reco_stats)]),
+    "raptr_matrix_drop_f32": (C.c_int, [VP]),
+    "raptr_matrix_bytes": (C.c_int, [VP, C.POINTER(C.c_int64)]),
+    "raptr_server_create": (C.c_int, [I32, C.POINTER(raptr_server_opts), C.POINTER(VP)]),
+    "raptr_server_destroy": (C.c_int, [VP]),
+    "raptr_server_submit": (C.c_int, [VP, C.POINTER(raptr_geom), I32, C.c_uint32, VP, I32, C.POINTER(C.c_int64)]),
+    "raptr_server_wait": (C.c_int, [VP, C.c_int64, VP, I32, C.POINTER(raptr_request_stats)]),
+    "raptr_server_get_stats": (C.c_int, [VP, C.POINTER(raptr_server_stats)]),
 }
 
 
@@ -463,6 +484,50 @@ class Context:
                                     niter, C.cast(ll, C.POINTER(C.c_double)) if loglik else None,
                                     _stream(stream)))
         return np.array(ll[:niter]) if loglik else None
+
+
+class Server:
+    """Serving loop (raptr_server): submit reconstructions of any geometry
+    at any time; they run with continuous batching on one GPU, with system
+    matrices cached in HBM."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 100 << 30, max_frames: int = 64,
+                 keep_fp32: bool = False):
+        o = raptr_server_opts(int(hbm_budget_bytes), int(max_frames), 1 if keep_fp32 else 0)
+        h = VP()
+        _check(lib().raptr_server_create(device, C.byref(o), C.byref(h)))
+        self._h = h
+
+    def submit(self, geom: Geometry, y, n_iter: int, nrays: int, seed: int) -> int:
+        """Queues a reconstruction; y holds float32 counts of all channels."""
+        y = np.ascontiguousarray(y, np.float32)
+        if y.size != geom.n_channels:
+            raise ValueError("y must hold one count per channel of the geometry")
+        gs = geom_struct(geom)
+        rid = C.c_int64(0)
+        _check(lib().raptr_server_submit(self._h, C.byref(gs), nrays, seed, y.ctypes.data, n_iter, C.byref(rid)))
+        return rid.value
+
+    def wait(self, rid: int, n_voxels: int, timeout_ms: int = -1):
+        """(image, stats) of a request; RaptrError on failure or timeout."""
+        x = np.empty(n_voxels, np.float32)
+        st = raptr_request_stats()
+        _check(lib().raptr_server_wait(self._h, rid, x.ctypes.data, timeout_ms, C.byref(st)))
+        return x, {k: getattr(st, k) for k, _ in raptr_request_stats._fields_}
+
+    def stats(self) -> dict:
+        st = raptr_server_stats()
+        _check(lib().raptr_server_get_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in raptr_server_stats._fields_}
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().raptr_server_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 # -- context-free operations ---------------------------------------------------

@@ -28,6 +28,7 @@ UNITS = {
     "kernels_transpose.cu": [],
     "kernels_precision.cu": [],
     "kernels_batch.cu": [],
+    "server.cu": [],
     "mlem_noalloc.cu": [],
 }
 

@@ -99,6 +99,10 @@ raptr_status validate_geom(const raptr_geom* g) {
 
 }  // namespace
 
+namespace raptr {
+raptr_status set_error(raptr_status st, const std::string& msg) { return fail(st, msg); }
+}  // namespace raptr
+
 // ---------------------------------------------------------------------------
 // Context and matrix objects
 // ---------------------------------------------------------------------------
@@ -1126,6 +1130,29 @@ raptr_status raptr_matrix_half_info(const raptr_matrix* A, uint16_t** d_hval, fl
   if (d_rscale) *d_rscale = A->rscale;
   if (d_htval) *d_htval = A->htval;
   if (d_pscale) *d_pscale = A->pscale;
+  return RAPTR_OK;
+}
+
+raptr_status raptr_matrix_drop_f32(raptr_matrix* A) {
+  if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
+  if (!A->hval) return fail(RAPTR_ERR_INVALID, "the FP32 values are the only ones: call raptr_matrix_half first");
+  DeviceScope ds(A->device);
+  cudaFree(A->val);
+  cudaFree(A->tval);
+  A->val = nullptr;
+  A->tval = nullptr;
+  return RAPTR_OK;
+}
+
+raptr_status raptr_matrix_bytes(const raptr_matrix* A, int64_t* bytes) {
+  if (!A || !bytes) return fail(RAPTR_ERR_INVALID, "bad argument");
+  const int64_t m = A->m, n = A->n, z = A->nnz;
+  int64_t b = (m + 1) * 8 + (A->col ? z * 4 : 0) + (A->val ? z * 4 : 0);
+  if (A->cp) b += (n + 1) * 8 + (A->trow ? z * 4 : 0) + (A->tval ? z * 4 : 0);
+  if (A->cnl) b += m * 4;
+  if (A->rank) b += m * 8;
+  if (A->hval) b += z * 4 + m * 8;
+  *bytes = b;
   return RAPTR_OK;
 }
 

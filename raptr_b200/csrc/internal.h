@@ -10,6 +10,9 @@
 
 namespace raptr {
 
+// Records msg as this thread's last error (raptr_last_error) and returns st.
+raptr_status set_error(raptr_status st, const std::string& msg);
+
 // Process-wide count of kernels launched by this library (diagnostic).
 void note_launches(long long k);
 long long launches_so_far();
