@@ -441,6 +441,91 @@ def batch_report(R, torch, ctx, w, lst, plain_iters_per_s, peak, n_frames=64, ni
     return out
 
 
+def serving_report(R, torch, rate_hz=20.0, window_s=8.0, budget_gb=120, seed=SEED + 500):
+    """The serving form: Poisson arrivals at rate_hz for window_s seconds of
+    reconstructions drawn from three geometries (40^3 x 2 mm / 5 angles,
+    70^3 x 2 mm / 180 angles, 100^3 x 1.5 mm / 60 angles), counts
+    log-uniform in [1e5, 1e8], iterations uniform in {10, 25, 50, 100}.
+    Matrices are built by the server on first use (warmed before the
+    window); latency is the server's submit-to-result time per request."""
+    rng = np.random.default_rng(seed)
+    kinds = [("small", cfg.WORKLOADS["small"]), ("full", cfg.WORKLOADS["full"]), ("fine", cfg.WORKLOADS["fine"])]
+    per_kind = 6
+    meas = {}
+    t_syn = time.perf_counter()
+    for name, w in kinds:
+        g = w["geom"]
+        ctx = R.Context(g, 0)
+        lst = torch.arange(g.n_channels, dtype=torch.int32, device="cuda")
+        A = ctx.build(lst, w["nrays"], SEED)
+        xt = torch.from_numpy(cfg.phantom(g, w.get("rods", False))).cuda()
+        lam = R.spmv(R.OP_N, A.m, A.n, A.row_ptr, A.col, A.val, xt)
+        del A, ctx
+        gc.collect()
+        lam = lam / lam.double().sum().float()
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed + len(meas))
+        meas[name] = []
+        for _ in range(per_kind):
+            counts = float(10 ** rng.uniform(5, 8))
+            meas[name].append((counts, torch.poisson(lam * counts, generator=gen).cpu().numpy()))
+        del lam
+        torch.cuda.empty_cache()
+    t_syn = time.perf_counter() - t_syn
+    srv = R.Server(0, hbm_budget_bytes=int(budget_gb) << 30)
+    warm = {}
+    for name, w in sorted(kinds, key=lambda kv: -kv[1]["geom"].n_channels):
+        g = w["geom"]
+        rid = srv.submit(g, meas[name][0][1], 10, w["nrays"], SEED)
+        _, st = srv.wait(rid, g.n_voxels)
+        warm[name] = st["total_ms"]
+    # arrivals
+    n_req = rng.poisson(rate_hz * window_s)
+    gaps = rng.exponential(1.0 / rate_hz, n_req)
+    picks = rng.integers(0, len(kinds), n_req)
+    which = rng.integers(0, per_kind, n_req)
+    iters = rng.choice([10, 25, 50, 100], n_req)
+    t0 = time.perf_counter()
+    sub = []
+    t_next = 0.0
+    for i in range(n_req):
+        t_next += gaps[i]
+        dt = t0 + t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        name, w = kinds[int(picks[i])]
+        counts, y = meas[name][int(which[i])]
+        sub.append((name, w["geom"], int(iters[i]), srv.submit(w["geom"], y, int(iters[i]), w["nrays"], SEED)))
+    results = []
+    for name, g, it, rid in sub:
+        _, st = srv.wait(rid, g.n_voxels)
+        results.append((name, it, st))
+    t_end = time.perf_counter()
+    stats = srv.stats()
+    srv.close()
+    lat = np.array([st["total_ms"] for _, _, st in results])
+    run = np.array([st["run_ms"] for _, _, st in results])
+    frame_iters = sum(it for _, it, _ in results)
+    by = {}
+    for name, _ in kinds:
+        l = np.array([st["total_ms"] for n_, _, st in results if n_ == name])
+        if l.size:
+            by[name] = {"requests": int(l.size), "p50_ms": float(np.percentile(l, 50)),
+                        "p99_ms": float(np.percentile(l, 99))}
+    return {
+        "offered_req_per_s": rate_hz, "window_s": window_s, "requests": int(n_req),
+        "completed_req_per_s": n_req / (t_end - t0), "frame_iterations_per_s": frame_iters / (t_end - t0),
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p95": float(np.percentile(lat, 95)),
+                       "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+        "run_ms": {"p50": float(np.percentile(run, 50)), "p99": float(np.percentile(run, 99))},
+        "by_geometry": by, "warm_first_request_ms": warm,
+        "server": {k: stats[k] for k in ("builds", "evictions", "batch_steps", "iterations")},
+        "largest_batch": int(max(st["frames_max"] for _, _, st in results)),
+        "hbm_budget_gb": budget_gb, "synthesis_s": t_syn,
+        "accuracy": "batched FP16 iteration; equal alone and in the mix and within 1e-3 of FP64 (tests/test_gpu_server.py)",
+    }
+
+
 def main():
     args = parse_args()
     w = workload(args.workload)
@@ -591,6 +676,11 @@ def main():
         peak, _ = measured_peaks()
         out["forms"] = {"precision": precision_report(R, torch, ctx, w, lst, y_dev, peak)}
         out["forms"]["batched"] = batch_report(R, torch, ctx, w, lst, out["resident_mlem_iters_per_s"], peak)
+        del lst, y_dev
+        gc.collect()
+        torch.cuda.empty_cache()
+        out["forms"]["serving"] = {"offered_20_per_s": serving_report(R, torch, rate_hz=20.0, window_s=8.0),
+                                   "offered_5_per_s": serving_report(R, torch, rate_hz=5.0, window_s=12.0)}
     if rank == 0 and world == 1:
         out["cpu_baseline"] = {k: v for k, v in cpu_job_rate(w, args.cpu_sample_s, os.cpu_count() or 1).items()
                                if k != "matrix_build_s"}

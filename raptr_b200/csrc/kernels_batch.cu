@@ -26,12 +26,17 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Blocks of a pass: one warp per item up to 64 blocks per SM, so that
+// blocks are short enough for the scheduler to interleave the kernels of
+// other streams (batches of other geometries served at the same time).
 unsigned grid_warps(int64_t items) {
   int64_t b = (items * 32 + kThreads - 1) / kThreads;
   if (b < 1) b = 1;
-  if (b > 148 * 8) b = 148 * 8;
+  if (b > 148 * 64) b = 148 * 64;
   return unsigned(b);
 }
+
+constexpr int kColsPerWarp = 48;  // back pass: columns a warp takes before its block ends
 
 __device__ __forceinline__ float to_f(float v) { return v; }
 __device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
@@ -124,8 +129,11 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
   double fsum[S::VEC];
 #pragma unroll
   for (int v = 0; v < S::VEC; v++) fsum[v] = 0.0;
+  __shared__ double red[KT];  // the block's image sums per frame of the tile
+  for (int i = threadIdx.x; i < KT; i += blockDim.x) red[i] = 0.0;
+  __syncthreads();
   (void)nw;
-  for (;;) {
+  for (int taken = 0; taken < kColsPerWarp; taken++) {
     // columns are handed out one at a time (their lengths vary ~20-fold)
     unsigned long long q = 0;
     if (lane == 0) q = atomicAdd(next, 1ull);
@@ -164,7 +172,10 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
   if (es == 0)
 #pragma unroll
     for (int v = 0; v < S::VEC; v++)
-      if (fsum[v] != 0.0) atomicAdd(acc + fbase + v, fsum[v]);
+      if (fsum[v] != 0.0) atomicAdd(red + (fbase - f0) + v, fsum[v]);
+  __syncthreads();
+  for (int i = threadIdx.x; i < KT; i += blockDim.x)
+    if (red[i] != 0.0) atomicAdd(acc + f0 + i, red[i]);
 }
 
 // X = XX * (1 / acc[f]) for all frames; then acc = 0 for the next pass.
@@ -187,7 +198,8 @@ cudaError_t launch_tile(bool forward, int64_t m, int64_t n, int K, int f0, const
     batch_forward_kernel<KT, VT><<<grid_warps(m), kThreads, 0, s>>>(m, K, f0, rp, col, static_cast<const VT*>(val),
                                                                     rscale, Y, X, rank, E);
   else
-    batch_back_kernel<KT, VT><<<grid_warps(n), kThreads, 0, s>>>(n, K, f0, next, cp, trow, static_cast<const VT*>(tval),
+    batch_back_kernel<KT, VT><<<unsigned((n + kColsPerWarp * (kThreads / 32) - 1) / (kColsPerWarp * (kThreads / 32))),
+                                kThreads, 0, s>>>(n, K, f0, next, cp, trow, static_cast<const VT*>(tval),
                                                                  E, X, S, col_order, XX, acc);
   note_launches(1);
   return cudaGetLastError();

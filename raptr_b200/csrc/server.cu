@@ -13,7 +13,9 @@
 // count; a finished image is copied to the host and the request's device
 // memory is returned.  Admission is by memory: a request waits while its
 // matrix plus the batch state would exceed the budget after evicting idle
-// matrices.
+// matrices.  Each geometry's batch advances as soon as its previous
+// iteration ends (end events are polled), so a small geometry is not held
+// to the pace of a large one.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -138,6 +140,12 @@ struct Entry {
   cudaStream_t stream = nullptr;
   std::vector<Request*> active;
   bool dirty = true;
+  // the iteration on the device: its end event and the requests in it
+  cudaEvent_t done_ev = nullptr;
+  bool in_flight = false;
+  raptr_status launch_status = RAPTR_OK;
+  std::string launch_error;
+  std::vector<Request*> members;
   float* X = nullptr;
   float* Y = nullptr;
   int K = 0;
@@ -195,7 +203,12 @@ raptr_status raptr_server::build(Entry* e, std::string* err) {
     *err = raptr_last_error();
     return st_;
   }
-  cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  // small geometries first when the device is shared: their iterations
+  // are short, so they should not queue behind a large batch's blocks
+  int lo = 0, hi = 0;
+  cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  cudaStreamCreateWithPriority(&e->stream, cudaStreamNonBlocking, channels_of(e->g) < (int64_t(1) << 20) ? hi : lo);
+  cudaEventCreateWithFlags(&e->done_ev, cudaEventDisableTiming);
   int32_t* lst = nullptr;
   const int64_t nch = channels_of(e->g);
   cudaError_t ce = cudaMalloc(&lst, size_t(nch) * sizeof(int32_t));
@@ -254,6 +267,8 @@ void raptr_server::drop(Entry* e) {
   if (e->A) raptr_matrix_destroy(e->A);
   if (e->ctx) raptr_ctx_destroy(e->ctx);
   if (e->stream) cudaStreamDestroy(e->stream);
+  if (e->done_ev) cudaEventDestroy(e->done_ev);
+  e->done_ev = nullptr;
   e->X = e->Y = e->s = nullptr;
   e->A = nullptr;
   e->ctx = nullptr;
@@ -408,85 +423,102 @@ void raptr_server::loop() {
   DeviceScope ds(device);
   std::unique_lock<std::mutex> lk(mu);
   for (;;) {
-    cv_work.wait(lk, [&] {
-      if (stop || !queue.empty()) return true;
+    auto busy = [&] {
       for (auto& kv : entries)
-        if (!kv.second->active.empty()) return true;
+        if (!kv.second->active.empty() || kv.second->in_flight) return true;
       return false;
-    });
+    };
+    cv_work.wait(lk, [&] { return stop || !queue.empty() || busy(); });
     if (stop) break;
     admit(lk);
-    std::vector<Entry*> work;
+    // every batch advances on its own: start an iteration wherever the
+    // device is idle for that geometry
+    std::vector<Entry*> start;
     for (auto& kv : entries)
-      if (!kv.second->active.empty()) work.push_back(kv.second.get());
-    if (work.empty()) {
-      if (!queue.empty()) cv_work.wait_for(lk, std::chrono::milliseconds(5));
-      continue;
+      if (!kv.second->in_flight && !kv.second->active.empty()) start.push_back(kv.second.get());
+    for (Entry* e : start) {
+      e->members = e->active;
+      e->in_flight = true;
     }
     lk.unlock();
-    // one iteration of every batch, each on its stream
-    std::vector<raptr_status> res(work.size(), RAPTR_OK);
-    std::vector<std::string> errs(work.size());
-    for (size_t i = 0; i < work.size(); i++) {
-      Entry* e = work[i];
+    for (Entry* e : start) {
+      e->launch_status = RAPTR_OK;
       if (e->dirty && relayout(e) != cudaSuccess) {
-        res[i] = RAPTR_ERR_NOMEM;
-        errs[i] = "batch relayout failed";
-        continue;
+        e->launch_status = RAPTR_ERR_NOMEM;
+        e->launch_error = "batch relayout failed";
+      } else {
+        // one sweep of the matrix for all frames (K is a power of two <= 64)
+        e->launch_status = raptr_mlem_batch(e->ctx, e->m, e->n, e->K, 1, e->rp, e->col, e->hval, e->rscale, e->cp,
+                                            e->trow, e->htval, e->rank, e->Y, e->s, e->X, 1, e->K, nullptr,
+                                            e->stream);
+        if (e->launch_status != RAPTR_OK) e->launch_error = raptr_last_error();
       }
-      // one sweep of the matrix for all frames (K is a power of two <= 64)
-      res[i] = raptr_mlem_batch(e->ctx, e->m, e->n, e->K, 1, e->rp, e->col, e->hval, e->rscale, e->cp, e->trow,
-                                e->htval, e->rank, e->Y, e->s, e->X, 1, e->K, nullptr, e->stream);
-      if (res[i] != RAPTR_OK) errs[i] = raptr_last_error();
+      cudaEventRecord(e->done_ev, e->stream);
     }
-    // finished images back to the host
-    std::vector<std::vector<std::pair<Request*, std::vector<float>>>> finished(work.size());
-    for (size_t i = 0; i < work.size(); i++) {
-      Entry* e = work[i];
-      cudaStreamSynchronize(e->stream);
-      if (res[i] != RAPTR_OK) continue;
-      float* tmp = nullptr;
-      for (Request* r : e->active) {
-        if (r->done + 1 < r->n_iter) continue;
-        if (!tmp && cudaMalloc(&tmp, size_t(e->n) * sizeof(float)) != cudaSuccess) break;
-        std::vector<float> x(size_t(e->n));
-        frame_extract_kernel<<<grid_of(e->n), 256, 0, e->stream>>>(e->n, e->K, r->slot, e->X, tmp);
-        note_launches(1);
-        cudaMemcpyAsync(x.data(), tmp, size_t(e->n) * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
-        cudaStreamSynchronize(e->stream);
-        finished[i].emplace_back(r, std::move(x));
+    // collect iterations that have ended; finished images to the host
+    std::vector<Entry*> ended;
+    std::vector<std::vector<std::pair<Request*, std::vector<float>>>> finished;
+    {
+      std::vector<Entry*> flying;
+      lk.lock();
+      for (auto& kv : entries)
+        if (kv.second->in_flight) flying.push_back(kv.second.get());
+      lk.unlock();
+      for (Entry* e : flying) {
+        if (cudaEventQuery(e->done_ev) != cudaSuccess) continue;
+        ended.push_back(e);
+        finished.emplace_back();
+        if (e->launch_status != RAPTR_OK) continue;
+        float* tmp = nullptr;
+        for (Request* r : e->members) {
+          if (r->done + 1 < r->n_iter) continue;
+          if (!tmp && cudaMalloc(&tmp, size_t(e->n) * sizeof(float)) != cudaSuccess) break;
+          std::vector<float> x(size_t(e->n));
+          frame_extract_kernel<<<grid_of(e->n), 256, 0, e->stream>>>(e->n, e->K, r->slot, e->X, tmp);
+          note_launches(1);
+          cudaMemcpyAsync(x.data(), tmp, size_t(e->n) * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
+          cudaStreamSynchronize(e->stream);
+          finished.back().emplace_back(r, std::move(x));
+        }
+        cudaFree(tmp);
       }
-      cudaFree(tmp);
+    }
+    if (ended.empty()) {
+      // nothing ended yet: give the device a moment
+      std::this_thread::sleep_for(std::chrono::microseconds(200));
+      lk.lock();
+      continue;
     }
     lk.lock();
-    for (size_t i = 0; i < work.size(); i++) {
-      Entry* e = work[i];
-      if (res[i] != RAPTR_OK) {
-        for (Request* r : e->active) {
+    for (size_t i = 0; i < ended.size(); i++) {
+      Entry* e = ended[i];
+      e->in_flight = false;
+      if (e->launch_status != RAPTR_OK) {
+        for (Request* r : e->members) {
+          if (r->state != 1) continue;
           cudaFree(r->y_dev);
           r->y_dev = nullptr;
           state_bytes -= e->m * 4;
           cache.unpin(r->key);
-          fail_request(r, res[i], errs[i]);
+          fail_request(r, e->launch_status, e->launch_error);
         }
-        e->active.clear();
-        e->dirty = true;
-        continue;
+      } else {
+        st.iterations += int64_t(e->members.size());
+        st.batch_steps++;
+        for (Request* r : e->members) r->done++;
+        for (auto& f : finished[i]) {
+          Request* r = f.first;
+          r->x_host = std::move(f.second);
+          r->state = 2;
+          r->t_done = Clock::now();
+          cudaFree(r->y_dev);
+          r->y_dev = nullptr;
+          state_bytes -= e->m * 4;
+          cache.unpin(r->key);
+          st.completed++;
+        }
       }
-      st.iterations += int64_t(e->active.size());
-      st.batch_steps++;
-      for (Request* r : e->active) r->done++;
-      for (auto& f : finished[i]) {
-        Request* r = f.first;
-        r->x_host = std::move(f.second);
-        r->state = 2;
-        r->t_done = Clock::now();
-        cudaFree(r->y_dev);
-        r->y_dev = nullptr;
-        state_bytes -= e->m * 4;
-        cache.unpin(r->key);
-        st.completed++;
-      }
+      e->members.clear();
       const size_t before = e->active.size();
       e->active.erase(std::remove_if(e->active.begin(), e->active.end(), [](Request* r) { return r->state != 1; }),
                       e->active.end());
