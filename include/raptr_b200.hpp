@@ -33,6 +33,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <memory>
@@ -42,6 +43,7 @@
 #include <vector>
 
 #include "raptr_b200.h"
+#include "raptr_b200_h5.h"
 
 #ifndef RAPTR_HD
 #if defined(__CUDACC__)
@@ -586,6 +588,107 @@ T sum(T* const& x, int const n) {
   double s = 0.0;
   raptr::check(raptr_sum(x, n, &s, nullptr), "raptr_sum");
   return T(s);
+}
+
+/* ------------------------------------------------------------------------ */
+/* HDF5 measurement and density files (src/H5Reader.hpp:34-102,               */
+/* src/H5DensityWriter.hpp:97-232, src/wrappers.hpp:330-482) over             */
+/* raptr_b200_h5.h                                                            */
+/* ------------------------------------------------------------------------ */
+
+namespace raptr {
+inline void check_h5(int st, const std::string& what) {
+  if (st != RAPTR_H5_OK) throw Exception(what + ": " + raptr_h5_last_error());
+}
+
+inline std::vector<float> read_dataset(std::string const& fn, const char* name) {
+  int64_t count = 0;
+  check_h5(raptr_h5_read_f32(fn.c_str(), name, nullptr, 0, &count), "read " + fn);
+  std::vector<float> v(static_cast<size_t>(count));
+  check_h5(raptr_h5_read_f32(fn.c_str(), name, v.data(), count, &count), "read " + fn);
+  return v;
+}
+}  // namespace raptr
+
+/* Reads the "messung" dataset of a measurement file (H5Reader::read). */
+class H5Reader {
+  std::string fn_;
+
+ public:
+  typedef float Value_t;
+  explicit H5Reader(std::string const& fn) : fn_(fn) {}
+  bool is_open() const {
+    int32_t rank = 0;
+    return raptr_h5_dataset_info(fn_.c_str(), "messung", &rank, nullptr) == RAPTR_H5_OK;
+  }
+  int sizeOfFile() const {
+    int64_t count = 0;
+    raptr::check_h5(raptr_h5_read_f32(fn_.c_str(), "messung", nullptr, 0, &count), "read " + fn_);
+    return int(count);
+  }
+  void read(Value_t* mem) const {
+    std::vector<float> v = raptr::read_dataset(fn_, "messung");
+    std::copy(v.begin(), v.end(), mem);
+  }
+};
+
+/* Writes the "density" dataset with the grid attributes. */
+template <typename TGrid>
+class H5DensityWriter {
+  std::string fn_;
+
+ public:
+  explicit H5DensityWriter(std::string const& fn) : fn_(fn) {}
+  void write(float const* mem, TGrid const& grid) const {
+    typename TGrid::CoordType o[3], d[3];
+    int n[3];
+    grid.getOrigin(o);
+    grid.getVoxelSize(d);
+    grid.getNumberOfVoxels(n);
+    float lo[3], hi[3];
+    for (int k = 0; k < 3; k++) {
+      lo[k] = static_cast<float>(o[k]);
+      hi[k] = lo[k] + n[k] * static_cast<float>(d[k]);
+    }
+    const int32_t nn[3] = {n[0], n[1], n[2]};
+    raptr::check_h5(raptr_h5_write_density(fn_.c_str(), mem, nn, lo, hi), "write " + fn_);
+  }
+};
+
+/* Nonzero counts of a measurement file as a sparse vector (channel ids in
+ * ascending order, values). */
+template <typename T>
+void readHDF5_MeasVct(std::vector<int>& vctId, std::vector<T>& vctVal, int& vctNnz, std::string const& ifn) {
+  std::vector<float> y = raptr::read_dataset(ifn, "messung");
+  vctId.clear();
+  vctVal.clear();
+  for (size_t i = 0; i < y.size(); i++)
+    if (y[i] != 0.f) {
+      vctId.push_back(int(i));
+      vctVal.push_back(T(y[i]));
+    }
+  vctNnz = int(vctId.size());
+}
+
+/* The measured channels of a measurement file (measurement list). */
+template <typename T>
+void readHDF5_MeasList(std::vector<int>& ml, int& mlN, std::string const& ifn) {
+  std::vector<T> v;
+  readHDF5_MeasVct(ml, v, mlN, ifn);
+}
+
+/* The density of a density file, x slowest. */
+template <typename T>
+std::vector<T> readHDF5_Density(std::string const& ifn) {
+  std::vector<float> d = raptr::read_dataset(ifn, "density");
+  return std::vector<T>(d.begin(), d.end());
+}
+
+template <typename T>
+void writeHDF5_Density(T const* const density, std::string const ofn, DefaultVoxelGrid<T> const& grid) {
+  static_assert(std::is_same<T, float>::value, "float only");
+  GridAdapter<DefaultVoxelGrid<T>, T> ga(&grid);
+  H5DensityWriter<GridAdapter<DefaultVoxelGrid<T>, T> >(ofn).write(density, ga);
 }
 
 #endif /* RAPTR_B200_HPP */

@@ -29,6 +29,7 @@ UNITS = {
     "kernels_precision.cu": [],
     "kernels_batch.cu": [],
     "server.cu": [],
+    "h5lite.cpp": [],
     "mlem_noalloc.cu": [],
 }
 
@@ -51,10 +52,11 @@ def build(verbose: bool = False, extra=()) -> str:
     os.makedirs(OBJ, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(HERE, "..", "include", "raptr_b200.h"))
+    headers.append(os.path.join(HERE, "..", "include", "raptr_b200_h5.h"))
     objs = []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)
-        obj = os.path.join(OBJ, unit.replace(".cu", ".o"))
+        obj = os.path.join(OBJ, os.path.splitext(unit)[0] + ".o")
         objs.append(obj)
         if _stale(obj, [src, __file__] + headers):
             cmd = [_nvcc(), "-c", src, "-o", obj] + ARCH + COMMON + flags + list(extra)
@@ -70,7 +72,34 @@ def build(verbose: bool = False, extra=()) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_drivers(headers)
     return LIB
+
+
+DRIVERS = ("reco", "backprojection", "pureSMCalculation")
+BIN = os.path.join(HERE, "bin")
+
+
+def build_drivers(headers=()) -> list:
+    """The command-line drivers (reference argv), host C++ over the
+    library: raptr_b200/bin/{reco,backprojection,pureSMCalculation}."""
+    os.makedirs(BIN, exist_ok=True)
+    src_dir = os.path.join(HERE, "drivers")
+    inc = os.path.join(HERE, "..", "include")
+    cuda = os.path.dirname(os.path.dirname(os.path.realpath(_nvcc()))) if os.path.sep in _nvcc() else "/usr/local/cuda"
+    out = []
+    for d in DRIVERS:
+        src = os.path.join(src_dir, d + ".cpp")
+        exe = os.path.join(BIN, d)
+        out.append(exe)
+        deps = [src, os.path.join(src_dir, "common.hpp"), LIB, os.path.join(inc, "raptr_b200.hpp")] + list(headers)
+        if _stale(exe, deps):
+            cmd = ["/usr/bin/g++", "-std=c++17", "-O2", src, "-o", exe, f"-I{inc}", f"-I{cuda}/include", f"-L{HERE}",
+                   "-lraptr_b200", f"-Wl,-rpath,{HERE}", f"-L{cuda}/lib64", "-lcudart", f"-Wl,-rpath,{cuda}/lib64"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"driver {d} failed to build:\n{r.stderr}")
+    return out
 
 
 if __name__ == "__main__":
