@@ -48,6 +48,16 @@ from raptr_b200 import config as cfg  # noqa: E402
 SEED = 1251
 MEAS_SEED = 20240
 
+# DRAM bytes per matrix entry of one launch, from the ncu capture of the
+# profile case (rows 0..299,999 of the full workload, 191,091,787 entries;
+# profiles/ncu_hot_kernels_profile_case.md): dram__bytes_read.sum +
+# dram__bytes_write.sum / entries.  The roofline's `traffic` scales them by
+# the entries of the timed matrix (traffic grows with the entries).
+TRAFFIC_BYTES_PER_ENTRY = {
+    "mlem_back_kernel": (1.541829e9 + 5.229568e6) / 191091787,
+    "mlem_forward_kernel": (1.534958e9 + 5.378560e6) / 191091787,
+}
+
 
 def parse_args():
     p = argparse.ArgumentParser()
@@ -647,11 +657,13 @@ def main():
             back_bytes = nnz * 8 + (n + 1) * 8 + 3 * n * 4 + m * 4
             r_f = fwd_bytes / (fwd_ms / 1e3) / 1e9
             r_b = back_bytes / (back_ms / 1e3) / 1e9
-            dom = ("mlem_back_kernel (column gather + update)", r_b, back_bytes, back_ms) if back_ms >= fwd_ms else \
-                ("mlem_forward_kernel (row SpMV + ratio)", r_f, fwd_bytes, fwd_ms)
+            dom = ("mlem_back_kernel", r_b, back_bytes, back_ms) if back_ms >= fwd_ms else \
+                ("mlem_forward_kernel", r_f, fwd_bytes, fwd_ms)
             out["roofline"] = {"bound": "hbm", "kernel": dom[0], "achieved": round(dom[1], 1), "peak": peak,
                                "unit": "GB/s", "frac": round(dom[1] / peak, 4), "peak_source": peak_kind,
-                               "traffic": None, "algorithmic_bytes": int(dom[2]), "launch_ms": round(dom[3], 4)}
+                               "traffic": int(TRAFFIC_BYTES_PER_ENTRY[dom[0]] * nnz),
+                               "traffic_source": "ncu DRAM bytes per entry of the profile case x entries",
+                               "algorithmic_bytes": int(dom[2]), "launch_ms": round(dom[3], 4)}
             out["roofline_all"] = {
                 "mlem_forward_kernel": {"achieved": round(r_f, 1), "frac": round(r_f / peak, 4),
                                         "bytes": int(fwd_bytes), "ms": round(fwd_ms, 4)},

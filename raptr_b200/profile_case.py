@@ -1,11 +1,14 @@
 """A small, self-contained case of the hot kernels for `ncu` captures.
 
-    python -m raptr_b200.profile_case [--rows R] [--workload full]
+    python -m raptr_b200.profile_case [--rows R] [--workload full] [--forms]
 
-Builds rows [0, R) of the workload's system matrix (one build chunk),
-transposes it and runs three MLEM iterations, so that each hot kernel
-(sm_rows_kernel, mlem_forward_kernel, mlem_back_kernel) launches a few times
-on a matrix larger than L2 but only a few GB on the device.
+Builds rows [0, R) of the workload's system matrix, transposes it (radix
+sort in the channels' back-projection order) and runs three MLEM
+iterations, so that each hot kernel (sm_rows_kernel, rs_scatter,
+mlem_forward_kernel, mlem_back_kernel) launches a few times on a matrix
+larger than L2 but only a few GB on the device.  With --forms it also runs
+the FP16 form (three iterations) and the batched form (16 frames, two
+iterations).
 """
 from __future__ import annotations
 
@@ -18,6 +21,7 @@ def main():
     p = argparse.ArgumentParser()
     p.add_argument("--rows", type=int, default=65536)
     p.add_argument("--workload", default="full")
+    p.add_argument("--forms", action="store_true")
     a = p.parse_args()
     import torch
 
@@ -35,6 +39,15 @@ def main():
     s64, s = R.sensitivity(A)
     x = torch.full((A.n,), np.float32(1.0 / A.n), device="cuda")
     ctx.mlem(A, y, s, x, 3, use_graph=False)
+    if a.forms:
+        A.to_half()
+        h64, h = R.sensitivity_half(A)
+        xh = torch.full((A.n,), np.float32(1.0 / A.n), device="cuda")
+        ctx.mlem_half(A, y, h, xh, 3, use_graph=False)
+        K = 16
+        Y = y.unsqueeze(1).repeat(1, K).contiguous()
+        X = torch.full((A.n, K), np.float32(1.0 / A.n), device="cuda")
+        ctx.mlem_batch(A, Y, h, X, 2, frame_tile=16, use_graph=False)
     torch.cuda.synchronize()
     print(f"profile case: {A.m} rows, {A.nnz} entries ({A.nnz * 8 / 1e9:.2f} GB CSR), x sum {float(x.sum()):.6f}")
 
