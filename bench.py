@@ -48,10 +48,10 @@ from raptr_b200 import config as cfg  # noqa: E402
 SEED = 1251
 MEAS_SEED = 20240
 
-# DRAM bytes per matrix entry of one launch, from the ncu capture of the
-# profile case (rows 0..299,999 of the full workload, 191,091,787 entries;
-# profiles/ncu_hot_kernels_profile_case.md): dram__bytes_read.sum +
-# dram__bytes_write.sum / entries.  The roofline's `traffic` scales them by
+# DRAM bytes per matrix entry of one launch, from an ncu capture of the
+# profile case (`python -m raptr_b200.profile_case --rows 300000 --forms`:
+# rows 0..299,999 of the full workload, 191,091,787 entries):
+# (dram__bytes_read.sum + dram__bytes_write.sum) / entries.  The roofline's `traffic` scales them by
 # the entries of the timed matrix (traffic grows with the entries).
 TRAFFIC_BYTES_PER_ENTRY = {
     "mlem_back_kernel": (1.541829e9 + 5.229568e6) / 191091787,
