@@ -39,6 +39,16 @@ __device__ __forceinline__ float plane_alpha(float o, float d, int i, float r0, 
   return RFDIV(RFSUB(RFADD(o, RFMUL(float(i), d)), r0), dir);
 }
 
+// RN(a / b) from y = RN(1 / b) (P. Markstein's correction, IBM J. R&D 34(1),
+// 1990), applied twice so that the first correction brings q within one ulp.
+__device__ __forceinline__ float div_rcp(float a, float b, float y) {
+  float q = __fmul_rn(a, y);
+  float r = __fmaf_rn(-q, b, a);
+  q = __fmaf_rn(r, y, q);
+  r = __fmaf_rn(-q, b, a);
+  return __fmaf_rn(r, y, q);
+}
+
 // Shared-memory accumulation table: keys (voxel id, -1 = empty) and sums.
 template <int H>
 struct RowTable {
@@ -74,9 +84,9 @@ struct RowTable {
 // of all three axes; a ray parallel to the planes of some axis (start and
 // end coordinate equal) leaves that axis unconstrained, as the reference's
 // masked min/max does, and every candidate voxel along it gets the length.
-template <class Emit>
+template <class Emit, class EmitKey>
 __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, const float r[6], Emit& emit,
-                                         int* bad_walk) {
+                                         EmitKey& emit_key, int* bad_walk) {
   float dir[3];
   bool s[3];
 #pragma unroll
@@ -139,6 +149,50 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
   }
   const bool all3 = s[0] && s[1] && s[2];
   const int guard_max = g.n[0] + g.n[1] + g.n[2] + 8;
+  if (all3) {
+    // One axis per step, chosen with selects (no runtime array index):
+    // the axis whose next plane comes first.  Planes of two axes at the same
+    // parameter take two steps; the voxel between them has zero length and
+    // is not emitted, as its reference value is zero.
+    int i0 = id[0], i1 = id[1], i2 = id[2];
+    float lo0 = lo[0], lo1 = lo[1], lo2 = lo[2];
+    float hi0 = hi[0], hi1 = hi[1], hi2 = hi[2];
+    const float y0 = __frcp_rn(dir[0]), y1 = __frcp_rn(dir[1]), y2 = __frcp_rn(dir[2]);
+    const int nyz = g.n[1] * g.n[2];
+    int key = i0 * nyz + i1 * g.n[2] + i2;
+    const int k0 = step[0] * nyz, k1 = step[1] * g.n[2], k2 = step[2];
+#pragma unroll 1
+    for (int it = 0; it < guard_max; it++) {
+      const float a_lo = fmaxf(lo0, fmaxf(lo1, lo2));
+      const float a_hi = fminf(hi0, fminf(hi1, hi2));
+      if (a_lo < a_hi) emit_key(key, RFMUL(RFSUB(a_hi, a_lo), len));
+      if (!(a_hi < amax_g)) return;
+      const bool ax = hi0 <= hi1 && hi0 <= hi2;
+      const bool ay = !ax && hi1 <= hi2;
+      const int st = ax ? step[0] : (ay ? step[1] : step[2]);
+      const int i = (ax ? i0 : (ay ? i1 : i2)) + st;
+      const int n = ax ? g.n[0] : (ay ? g.n[1] : g.n[2]);
+      if (unsigned(i) >= unsigned(n)) return;
+      const float o = ax ? g.o[0] : (ay ? g.o[1] : g.o[2]);
+      const float pd = ax ? g.d[0] : (ay ? g.d[1] : g.d[2]);
+      const float r0 = ax ? r[0] : (ay ? r[1] : r[2]);
+      const float dd = ax ? dir[0] : (ay ? dir[1] : dir[2]);
+      const float yy = ax ? y0 : (ay ? y1 : y2);
+      const float hn = div_rcp(RFSUB(RFADD(o, RFMUL(float(st > 0 ? i + 1 : i), pd)), r0), dd, yy);
+      key += ax ? k0 : (ay ? k1 : k2);
+      i0 = ax ? i : i0;
+      i1 = ay ? i : i1;
+      i2 = (!ax && !ay) ? i : i2;
+      lo0 = ax ? a_hi : lo0;
+      lo1 = ay ? a_hi : lo1;
+      lo2 = (!ax && !ay) ? a_hi : lo2;
+      hi0 = ax ? hn : hi0;
+      hi1 = ay ? hn : hi1;
+      hi2 = (!ax && !ay) ? hn : hi2;
+    }
+    *bad_walk = 1;
+    return;
+  }
 #pragma unroll 1
   for (int it = 0; it < guard_max; it++) {
     float a_lo = fmaxf(lo[0], fmaxf(lo[1], lo[2]));
@@ -242,6 +296,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
   const int nyz = g.n[1] * g.n[2];
   const int nz = g.n[2];
   auto emit = [&](int ix, int iy, int iz, float L) { table.add(ix * nyz + iy * nz + iz, L); };
+  auto emit_key = [&](int key, float L) { table.add(key, L); };
   for (int ray = tid; ray < nrays; ray += T) {
     float r[6];
     if (rays) {
@@ -251,7 +306,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     } else {
       make_ray(ch, seed, cnl, ray, r);
     }
-    walk_ray(g, ch, r, emit, &bad_walk);
+    walk_ray(g, ch, r, emit, emit_key, &bad_walk);
   }
   __syncthreads();
 
