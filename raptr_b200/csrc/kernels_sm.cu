@@ -85,7 +85,7 @@ struct RowTable {
 // end coordinate equal) leaves that axis unconstrained, as the reference's
 // masked min/max does, and every candidate voxel along it gets the length.
 template <class Emit, class EmitKey>
-__device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, const float r[6], Emit& emit,
+__device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, const float r[6], int part, Emit& emit,
                                          EmitKey& emit_key, int* bad_walk) {
   float dir[3];
   bool s[3];
@@ -161,18 +161,115 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
     const int nyz = g.n[1] * g.n[2];
     int key = i0 * nyz + i1 * g.n[2] + i2;
     const int k0 = step[0] * nyz, k1 = step[1] * g.n[2], k2 = step[2];
+    // Staggered start: the walk begins at a plane of the dominant axis D,
+    // part/256 of the way along the ray, runs to the exit, then wraps
+    // around to the entry and runs up to that plane.  No voxel straddles a
+    // plane of D, so every voxel is still visited once with the same
+    // lengths, while the threads of a row -- nearly parallel rays of one
+    // channel -- sit on different voxels at any step instead of adding to
+    // the same shared-memory accumulator at once.
+    const int s0 = i0, s1 = i1, s2 = i2, skey = key;
+    const float sl0 = lo0, sl1 = lo1, sl2 = lo2, sh0 = hi0, sh1 = hi1, sh2 = hi2;
+    float stop = amax_g, a_split = amax_g;
+    bool wrapped = true;
+    if (part > 0) {
+      const float dx = fabsf(dir[0]), dy = fabsf(dir[1]), dz = fabsf(dir[2]);
+      const int D = (dx >= dy) ? ((dx >= dz) ? 0 : 2) : ((dy >= dz) ? 1 : 2);
+      const float oD = D == 0 ? g.o[0] : (D == 1 ? g.o[1] : g.o[2]);
+      const float pD = D == 0 ? g.d[0] : (D == 1 ? g.d[1] : g.d[2]);
+      const float rD = D == 0 ? r[0] : (D == 1 ? r[1] : r[2]);
+      const float dD = D == 0 ? dir[0] : (D == 1 ? dir[1] : dir[2]);
+      const int stD = D == 0 ? step[0] : (D == 1 ? step[1] : step[2]);
+      const int nD = D == 0 ? g.n[0] : (D == 1 ? g.n[1] : g.n[2]);
+      const int iD = D == 0 ? i0 : (D == 1 ? i1 : i2);
+      const float hD = D == 0 ? hi0 : (D == 1 ? hi1 : hi2);
+      const int span = int(fabsf((amax_g - amin_g) * dD) / pD) + 1;
+      const int k = (part * span) >> 8;
+      const int is = iD + stD * k;
+      if (k > 0 && is >= 0 && is < nD) {
+        const float as = plane_alpha(oD, pD, stD > 0 ? is : is + 1, rD, dD);
+        if (as > hD && as < amax_g) {
+          int ni[3];
+          float nl[3], nh[3];
+          bool ok = true;
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            if (d == D) {
+              ni[d] = is;
+              nl[d] = as;
+              nh[d] = plane_alpha(oD, pD, stD > 0 ? is + 1 : is, rD, dD);
+            } else {
+              // the voxel of axis d whose interval [lo, hi) holds as
+              int i = int(floorf((r[d] + as * dir[d] - g.o[d]) / g.d[d]));
+              i = min(max(i, 0), g.n[d] - 1);
+              float l = 0.f, h = 0.f;
+              bool found = false;
+#pragma unroll 1
+              for (int guard = 0; guard < 64 && !found; guard++) {
+                const float pa = plane_alpha(g.o[d], g.d[d], i, r[d], dir[d]);
+                const float pb = plane_alpha(g.o[d], g.d[d], i + 1, r[d], dir[d]);
+                l = step[d] > 0 ? pa : pb;
+                h = step[d] > 0 ? pb : pa;
+                if (!(h > as))
+                  i += step[d];
+                else if (l > as)
+                  i -= step[d];
+                else
+                  found = true;
+                if (i < 0 || i >= g.n[d]) break;
+              }
+              ok = ok && found;
+              ni[d] = i;
+              nl[d] = l;
+              nh[d] = h;
+            }
+          }
+          if (ok) {
+            i0 = ni[0];
+            i1 = ni[1];
+            i2 = ni[2];
+            lo0 = nl[0];
+            lo1 = nl[1];
+            lo2 = nl[2];
+            hi0 = nh[0];
+            hi1 = nh[1];
+            hi2 = nh[2];
+            key = i0 * nyz + i1 * g.n[2] + i2;
+            a_split = as;
+            wrapped = false;
+          }
+        }
+      }
+    }
 #pragma unroll 1
     for (int it = 0; it < guard_max; it++) {
       const float a_lo = fmaxf(lo0, fmaxf(lo1, lo2));
       const float a_hi = fminf(hi0, fminf(hi1, hi2));
       if (a_lo < a_hi) emit_key(key, RFMUL(RFSUB(a_hi, a_lo), len));
-      if (!(a_hi < amax_g)) return;
+      bool leave = !(a_hi < stop);
       const bool ax = hi0 <= hi1 && hi0 <= hi2;
       const bool ay = !ax && hi1 <= hi2;
       const int st = ax ? step[0] : (ay ? step[1] : step[2]);
       const int i = (ax ? i0 : (ay ? i1 : i2)) + st;
       const int n = ax ? g.n[0] : (ay ? g.n[1] : g.n[2]);
-      if (unsigned(i) >= unsigned(n)) return;
+      leave = leave || unsigned(i) >= unsigned(n);
+      if (leave) {
+        if (wrapped) return;
+        // the second leg: from the entry up to the split plane
+        i0 = s0;
+        i1 = s1;
+        i2 = s2;
+        lo0 = sl0;
+        lo1 = sl1;
+        lo2 = sl2;
+        hi0 = sh0;
+        hi1 = sh1;
+        hi2 = sh2;
+        key = skey;
+        stop = a_split;
+        wrapped = true;
+        continue;
+      }
       const float o = ax ? g.o[0] : (ay ? g.o[1] : g.o[2]);
       const float pd = ax ? g.d[0] : (ay ? g.d[1] : g.d[2]);
       const float r0 = ax ? r[0] : (ay ? r[1] : r[2]);
@@ -306,7 +403,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     } else {
       make_ray(ch, seed, cnl, ray, r);
     }
-    walk_ray(g, ch, r, emit, emit_key, &bad_walk);
+    walk_ray(g, ch, r, int(threadIdx.x) & 255, emit, emit_key, &bad_walk);
   }
   __syncthreads();
 
