@@ -403,7 +403,9 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     } else {
       make_ray(ch, seed, cnl, ray, r);
     }
-    walk_ray(g, ch, r, int(threadIdx.x) & 255, emit, emit_key, &bad_walk);
+    // start offsets: the thread index bit-reversed, so that neighbouring
+    // lanes start far apart along the ray
+    walk_ray(g, ch, r, int(__brev(threadIdx.x) >> 24), emit, emit_key, &bad_walk);
   }
   __syncthreads();
 
