@@ -285,9 +285,11 @@ def synth_measurement(R, torch, ctx, w, lst, dist=None):
     return cfg.poisson_measurement(lam.cpu().numpy(), w["counts"], MEAS_SEED)
 
 
-def run_job(R, torch, ctx, w, lst, y_dev, dist=None):
-    """One reconstruction job; returns per-phase device times (ms) and the
-    per-iteration kernel times."""
+def run_job(R, torch, ctx, w, lst, y_dev, dist=None, keep=False):
+    """One reconstruction job; returns per-phase device times (ms), and with
+    keep the matrix and the inputs of its iterations (for kernel timing
+    after the timed region).  On one GPU the iterations run as one CUDA
+    graph."""
     g = w["geom"]
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
     ev[0].record()
@@ -304,8 +306,9 @@ def run_job(R, torch, ctx, w, lst, y_dev, dist=None):
         s = sharded.sensitivity()
     ev[3].record()
     x = torch.full((g.n_voxels,), np.float32(1.0 / g.n_voxels), device="cuda")
+    kt = None
     if dist is None:
-        kt = ctx.mlem(A, y_dev, s, x, w["niter"], use_graph=False, kernel_times=True)
+        ctx.mlem(A, y_dev, s, x, w["niter"], use_graph=True)
     else:
         ops = sharded.ops
         kev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(w["niter"])]
@@ -323,6 +326,8 @@ def run_job(R, torch, ctx, w, lst, y_dev, dist=None):
     torch.cuda.synchronize()
     t = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
     info = {"nnz": A.nnz, "m": A.m}
+    if keep:
+        info.update({"A": A, "s": s})
     del A
     gc.collect()
     return {"build_ms": t[0], "transpose_ms": t[1], "sens_ms": t[2], "mlem_ms": t[3], "job_ms": sum(t),
@@ -609,12 +614,21 @@ def main():
     t_end = torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("raptr_timed_steps")
     t_start.record()
-    steps = [run_job(R, torch, ctx, w, lst, y_dev, dist) for _ in range(args.steps)]
+    steps = [run_job(R, torch, ctx, w, lst, y_dev, dist, keep=(i == args.steps - 1)) for i in range(args.steps)]
     t_end.record()
     torch.cuda.nvtx.range_pop()
     barrier()
     launches = R.kernel_launches() - launches0
     clocks = sampler.stop()
+    # per-pass device times of the iteration, on the last step's matrix,
+    # outside the timed region (events between the passes)
+    last = steps[-1]
+    if dist is None and "A" in last:
+        last["kernel_ms"] = ctx.mlem(last["A"], y_dev, last["s"], last["x"].clone(), 10, use_graph=False,
+                                     kernel_times=True)
+    last.pop("A", None)
+    last.pop("s", None)
+    gc.collect()
     total_ms = t_start.elapsed_time(t_end)
     if dist is not None:
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
@@ -649,7 +663,7 @@ def main():
         # Roofline of the HBM-bound MLEM passes, from the per-kernel device
         # times of the timed steps.
         peak, peak_kind = measured_peaks()
-        kts = np.concatenate([s["kernel_ms"] for s in steps])
+        kts = np.concatenate([s["kernel_ms"] for s in steps if s["kernel_ms"] is not None])
         if np.all(np.isfinite(kts)):
             fwd_ms, back_ms = float(kts[:, 0].mean()), float(kts[:, 1].mean())
             n = g.n_voxels

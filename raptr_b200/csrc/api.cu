@@ -985,9 +985,8 @@ raptr_status mlem_impl(raptr_ctx* ctx, int64_t m, int64_t n, const MlemArrays& A
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (e == cudaSuccess) e = cudaGraphLaunch(exec, cap);
-    // the captured launches were counted once at capture; replaying the
-    // graph launches them again
-    if (e == cudaSuccess) note_launches(3LL * n_iter);
+    // the launches were counted when they were captured; the graph runs
+    // each of them once
     if (e == cudaSuccess) e = cudaEventRecord(ev, cap);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cap);
@@ -1268,17 +1267,14 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
     if (e == cudaSuccess) e = cudaStreamWaitEvent(cap, ev, 0);
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    const long long before = launches_so_far();
     if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       cudaError_t e1 = enqueue(cap);
       cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
       e = (e1 != cudaSuccess) ? e1 : e2;
     }
-    const long long captured = launches_so_far() - before;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (e == cudaSuccess) e = cudaGraphLaunch(exec, cap);
-    if (e == cudaSuccess) note_launches(captured);  // the replay launches them again
     if (e == cudaSuccess) e = cudaEventRecord(ev, cap);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cap);
