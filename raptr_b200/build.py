@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import os
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -53,20 +54,27 @@ def build(verbose: bool = False, extra=()) -> str:
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(HERE, "..", "include", "raptr_b200.h"))
     headers.append(os.path.join(HERE, "..", "include", "raptr_b200_h5.h"))
-    objs = []
+    objs, jobs = [], []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(OBJ, os.path.splitext(unit)[0] + ".o")
         objs.append(obj)
         if _stale(obj, [src, __file__] + headers):
-            cmd = [_nvcc(), "-c", src, "-o", obj] + ARCH + COMMON + flags + list(extra)
-            if verbose:
-                print(" ".join(cmd))
-            r = subprocess.run(cmd, capture_output=True, text=True)
-            if r.returncode != 0:
-                raise RuntimeError(f"nvcc failed for {unit}:\n{r.stdout}\n{r.stderr}")
-            if verbose and (r.stdout or r.stderr):
-                print(r.stdout, r.stderr)
+            jobs.append((unit, [_nvcc(), "-c", src, "-o", obj] + ARCH + COMMON + flags + list(extra)))
+
+    def compile_unit(job):
+        unit, cmd = job
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {unit}:\n{r.stdout}\n{r.stderr}")
+        if verbose and (r.stdout or r.stderr):
+            print(r.stdout, r.stderr)
+
+    # the translation units compile independently
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        list(pool.map(compile_unit, jobs))
     if _stale(LIB, objs):
         cmd = [_nvcc(), "-shared", "-o", LIB] + objs + ARCH + ["-ccbin", "/usr/bin/g++"]
         r = subprocess.run(cmd, capture_output=True, text=True)
