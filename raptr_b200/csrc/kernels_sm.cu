@@ -49,6 +49,15 @@ __device__ __forceinline__ float div_rcp(float a, float b, float y) {
   return __fmaf_rn(r, y, q);
 }
 
+// plane_alpha with the division by a precomputed reciprocal rc = RN(1/dir)
+// (exact as RN(num/dir), see div_rcp); a dir whose reciprocal is not a
+// normal float takes the division itself.
+__device__ __forceinline__ float plane_alpha_r(float o, float d, int i, float r0, float dir, float rc) {
+  const float num = RFSUB(RFADD(o, RFMUL(float(i), d)), r0);
+  if (!(fabsf(dir) >= 1e-30f && fabsf(dir) <= 1e30f)) return RFDIV(num, dir);
+  return div_rcp(num, dir, rc);
+}
+
 // Shared-memory accumulation table: keys (voxel id, -1 = empty) and sums.
 template <int H>
 struct RowTable {
@@ -95,6 +104,9 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
     s[d] = r[d] != r[3 + d];
   }
   if (!(s[0] || s[1] || s[2])) return;
+  float rc[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) rc[d] = s[d] ? __frcp_rn(dir[d]) : 0.f;
   const float len = norm3_exact(dir[0], dir[1], dir[2]);
   int step[3] = {0, 0, 0};
   float amin_g = -INFINITY, amax_g = INFINITY;
@@ -102,8 +114,8 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
   for (int d = 0; d < 3; d++) {
     if (s[d]) {
       step[d] = (r[3 + d] > r[d]) ? 1 : -1;
-      float a0 = plane_alpha(g.o[d], g.d[d], 0, r[d], dir[d]);
-      float a1 = plane_alpha(g.o[d], g.d[d], g.n[d], r[d], dir[d]);
+      float a0 = plane_alpha_r(g.o[d], g.d[d], 0, r[d], dir[d], rc[d]);
+      float a1 = plane_alpha_r(g.o[d], g.d[d], g.n[d], r[d], dir[d], rc[d]);
       amin_g = fmaxf(amin_g, fminf(a0, a1));
       amax_g = fminf(amax_g, fmaxf(a0, a1));
     }
@@ -126,8 +138,8 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
       float l, h;
 #pragma unroll 1
       for (int guard = 0; guard < 64; guard++) {
-        float pa = plane_alpha(g.o[d], g.d[d], i, r[d], dir[d]);
-        float pb = plane_alpha(g.o[d], g.d[d], i + 1, r[d], dir[d]);
+        float pa = plane_alpha_r(g.o[d], g.d[d], i, r[d], dir[d], rc[d]);
+        float pb = plane_alpha_r(g.o[d], g.d[d], i + 1, r[d], dir[d], rc[d]);
         l = step[d] > 0 ? pa : pb;
         h = step[d] > 0 ? pb : pa;
         if (!(h > amin_g)) {
@@ -157,7 +169,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
     int i0 = id[0], i1 = id[1], i2 = id[2];
     float lo0 = lo[0], lo1 = lo[1], lo2 = lo[2];
     float hi0 = hi[0], hi1 = hi[1], hi2 = hi[2];
-    const float y0 = __frcp_rn(dir[0]), y1 = __frcp_rn(dir[1]), y2 = __frcp_rn(dir[2]);
+    const float y0 = rc[0], y1 = rc[1], y2 = rc[2];
     const int nyz = g.n[1] * g.n[2];
     int key = i0 * nyz + i1 * g.n[2] + i2;
     const int k0 = step[0] * nyz, k1 = step[1] * g.n[2], k2 = step[2];
@@ -179,6 +191,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
       const float pD = D == 0 ? g.d[0] : (D == 1 ? g.d[1] : g.d[2]);
       const float rD = D == 0 ? r[0] : (D == 1 ? r[1] : r[2]);
       const float dD = D == 0 ? dir[0] : (D == 1 ? dir[1] : dir[2]);
+      const float cD = D == 0 ? rc[0] : (D == 1 ? rc[1] : rc[2]);
       const int stD = D == 0 ? step[0] : (D == 1 ? step[1] : step[2]);
       const int nD = D == 0 ? g.n[0] : (D == 1 ? g.n[1] : g.n[2]);
       const int iD = D == 0 ? i0 : (D == 1 ? i1 : i2);
@@ -187,7 +200,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
       const int k = (part * span) >> 8;
       const int is = iD + stD * k;
       if (k > 0 && is >= 0 && is < nD) {
-        const float as = plane_alpha(oD, pD, stD > 0 ? is : is + 1, rD, dD);
+        const float as = plane_alpha_r(oD, pD, stD > 0 ? is : is + 1, rD, dD, cD);
         if (as > hD && as < amax_g) {
           int ni[3];
           float nl[3], nh[3];
@@ -197,7 +210,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
             if (d == D) {
               ni[d] = is;
               nl[d] = as;
-              nh[d] = plane_alpha(oD, pD, stD > 0 ? is + 1 : is, rD, dD);
+              nh[d] = plane_alpha_r(oD, pD, stD > 0 ? is + 1 : is, rD, dD, cD);
             } else {
               // the voxel of axis d whose interval [lo, hi) holds as
               int i = int(floorf((r[d] + as * dir[d] - g.o[d]) / g.d[d]));
@@ -206,8 +219,8 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
               bool found = false;
 #pragma unroll 1
               for (int guard = 0; guard < 64 && !found; guard++) {
-                const float pa = plane_alpha(g.o[d], g.d[d], i, r[d], dir[d]);
-                const float pb = plane_alpha(g.o[d], g.d[d], i + 1, r[d], dir[d]);
+                const float pa = plane_alpha_r(g.o[d], g.d[d], i, r[d], dir[d], rc[d]);
+                const float pb = plane_alpha_r(g.o[d], g.d[d], i + 1, r[d], dir[d], rc[d]);
                 l = step[d] > 0 ? pa : pb;
                 h = step[d] > 0 ? pb : pa;
                 if (!(h > as))
@@ -241,51 +254,57 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
         }
       }
     }
+    // Loop state per axis: the parameter of the next plane (hi) and the index
+    // of the plane after it, as a float (exact small integers).  The entry
+    // parameter of the current voxel is the previous step's exit (prev).
+    const float f0 = float(step[0]), f1 = float(step[1]), f2 = float(step[2]);
+    float q0 = float(step[0] > 0 ? i0 + 2 : i0 - 1);
+    float q1 = float(step[1] > 0 ? i1 + 2 : i1 - 1);
+    float q2 = float(step[2] > 0 ? i2 + 2 : i2 - 1);
+    float prev = fmaxf(lo0, fmaxf(lo1, lo2));
+    const float sq0 = float(step[0] > 0 ? s0 + 2 : s0 - 1);
+    const float sq1 = float(step[1] > 0 ? s1 + 2 : s1 - 1);
+    const float sq2 = float(step[2] > 0 ? s2 + 2 : s2 - 1);
+    const float sprev = fmaxf(sl0, fmaxf(sl1, sl2));
 #pragma unroll 1
     for (int it = 0; it < guard_max; it++) {
-      const float a_lo = fmaxf(lo0, fmaxf(lo1, lo2));
       const float a_hi = fminf(hi0, fminf(hi1, hi2));
-      if (a_lo < a_hi) emit_key(key, RFMUL(RFSUB(a_hi, a_lo), len));
-      bool leave = !(a_hi < stop);
-      const bool ax = hi0 <= hi1 && hi0 <= hi2;
-      const bool ay = !ax && hi1 <= hi2;
-      const int st = ax ? step[0] : (ay ? step[1] : step[2]);
-      const int i = (ax ? i0 : (ay ? i1 : i2)) + st;
-      const int n = ax ? g.n[0] : (ay ? g.n[1] : g.n[2]);
-      leave = leave || unsigned(i) >= unsigned(n);
-      if (leave) {
+      if (prev < a_hi) emit_key(key, RFMUL(RFSUB(a_hi, prev), len));
+      // The next plane lies before the exit, so it is not the grid's last
+      // plane of its axis, and the step stays inside the grid.
+      if (!(a_hi < stop)) {
         if (wrapped) return;
         // the second leg: from the entry up to the split plane
-        i0 = s0;
-        i1 = s1;
-        i2 = s2;
-        lo0 = sl0;
-        lo1 = sl1;
-        lo2 = sl2;
+        q0 = sq0;
+        q1 = sq1;
+        q2 = sq2;
         hi0 = sh0;
         hi1 = sh1;
         hi2 = sh2;
         key = skey;
+        prev = sprev;
         stop = a_split;
         wrapped = true;
         continue;
       }
+      const bool ax = hi0 == a_hi;
+      const bool ay = !ax && hi1 == a_hi;
+      const float q = ax ? q0 : (ay ? q1 : q2);
       const float o = ax ? g.o[0] : (ay ? g.o[1] : g.o[2]);
       const float pd = ax ? g.d[0] : (ay ? g.d[1] : g.d[2]);
       const float r0 = ax ? r[0] : (ay ? r[1] : r[2]);
       const float dd = ax ? dir[0] : (ay ? dir[1] : dir[2]);
       const float yy = ax ? y0 : (ay ? y1 : y2);
-      const float hn = div_rcp(RFSUB(RFADD(o, RFMUL(float(st > 0 ? i + 1 : i), pd)), r0), dd, yy);
+      const float hn = div_rcp(RFSUB(RFADD(o, RFMUL(q, pd)), r0), dd, yy);
+      const float qn = q + (ax ? f0 : (ay ? f1 : f2));
       key += ax ? k0 : (ay ? k1 : k2);
-      i0 = ax ? i : i0;
-      i1 = ay ? i : i1;
-      i2 = (!ax && !ay) ? i : i2;
-      lo0 = ax ? a_hi : lo0;
-      lo1 = ay ? a_hi : lo1;
-      lo2 = (!ax && !ay) ? a_hi : lo2;
+      q0 = ax ? qn : q0;
+      q1 = ay ? qn : q1;
+      q2 = (!ax && !ay) ? qn : q2;
       hi0 = ax ? hn : hi0;
       hi1 = ay ? hn : hi1;
       hi2 = (!ax && !ay) ? hn : hi2;
+      prev = a_hi;
     }
     *bad_walk = 1;
     return;
