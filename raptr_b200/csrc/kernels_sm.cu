@@ -93,7 +93,7 @@ struct RowTable {
 // of all three axes; a ray parallel to the planes of some axis (start and
 // end coordinate equal) leaves that axis unconstrained, as the reference's
 // masked min/max does, and every candidate voxel along it gets the length.
-template <class Emit, class EmitKey>
+template <bool OISO, class Emit, class EmitKey>
 __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, const float r[6], int part, Emit& emit,
                                          EmitKey& emit_key, int* bad_walk) {
   float dir[3];
@@ -164,8 +164,8 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
   if (all3) {
     // One axis per step, chosen with selects (no runtime array index):
     // the axis whose next plane comes first.  Planes of two axes at the same
-    // parameter take two steps; the voxel between them has zero length and
-    // is not emitted, as its reference value is zero.
+    // parameter take two steps; the voxel between them has zero length (its
+    // reference value is zero) and is dropped when the row is compacted.
     int i0 = id[0], i1 = id[1], i2 = id[2];
     float lo0 = lo[0], lo1 = lo[1], lo2 = lo[2];
     float hi0 = hi[0], hi1 = hi[1], hi2 = hi[2];
@@ -255,21 +255,29 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
       }
     }
     // Loop state per axis: the parameter of the next plane (hi) and the index
-    // of the plane after it, as a float (exact small integers).  The entry
-    // parameter of the current voxel is the previous step's exit (prev).
-    const float f0 = float(step[0]), f1 = float(step[1]), f2 = float(step[2]);
-    float q0 = float(step[0] > 0 ? i0 + 2 : i0 - 1);
-    float q1 = float(step[1] > 0 ? i1 + 2 : i1 - 1);
-    float q2 = float(step[2] > 0 ? i2 + 2 : i2 - 1);
+    // of the plane after it times the step direction, as a float (exact
+    // small integers), so that it grows by one per step on every axis; the
+    // pitch carries the direction instead (q*pd = (-q)*(-pd) exactly).  The
+    // entry parameter of the current voxel is the previous step's exit
+    // (prev).
+    const float ps0 = step[0] > 0 ? g.d[0] : -g.d[0];
+    const float ps1 = step[1] > 0 ? g.d[1] : -g.d[1];
+    const float ps2 = step[2] > 0 ? g.d[2] : -g.d[2];
+    float q0 = float(step[0] > 0 ? i0 + 2 : 1 - i0);
+    float q1 = float(step[1] > 0 ? i1 + 2 : 1 - i1);
+    float q2 = float(step[2] > 0 ? i2 + 2 : 1 - i2);
     float prev = fmaxf(lo0, fmaxf(lo1, lo2));
-    const float sq0 = float(step[0] > 0 ? s0 + 2 : s0 - 1);
-    const float sq1 = float(step[1] > 0 ? s1 + 2 : s1 - 1);
-    const float sq2 = float(step[2] > 0 ? s2 + 2 : s2 - 1);
+    const float sq0 = float(step[0] > 0 ? s0 + 2 : 1 - s0);
+    const float sq1 = float(step[1] > 0 ? s1 + 2 : 1 - s1);
+    const float sq2 = float(step[2] > 0 ? s2 + 2 : 1 - s2);
     const float sprev = fmaxf(sl0, fmaxf(sl1, sl2));
 #pragma unroll 1
     for (int it = 0; it < guard_max; it++) {
       const float a_hi = fminf(hi0, fminf(hi1, hi2));
-      if (prev < a_hi) emit_key(key, RFMUL(RFSUB(a_hi, prev), len));
+      // A voxel between two planes at the same parameter gets length 0; it
+      // is added all the same (no branch) and dropped with the other
+      // zero sums when the row is compacted.
+      emit_key(key, RFMUL(RFSUB(a_hi, prev), len));
       // The next plane lies before the exit, so it is not the grid's last
       // plane of its axis, and the step stays inside the grid.
       if (!(a_hi < stop)) {
@@ -290,13 +298,13 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
       const bool ax = hi0 == a_hi;
       const bool ay = !ax && hi1 == a_hi;
       const float q = ax ? q0 : (ay ? q1 : q2);
-      const float o = ax ? g.o[0] : (ay ? g.o[1] : g.o[2]);
-      const float pd = ax ? g.d[0] : (ay ? g.d[1] : g.d[2]);
+      const float o = OISO ? g.o[0] : (ax ? g.o[0] : (ay ? g.o[1] : g.o[2]));
+      const float pd = ax ? ps0 : (ay ? ps1 : ps2);
       const float r0 = ax ? r[0] : (ay ? r[1] : r[2]);
       const float dd = ax ? dir[0] : (ay ? dir[1] : dir[2]);
       const float yy = ax ? y0 : (ay ? y1 : y2);
       const float hn = div_rcp(RFSUB(RFADD(o, RFMUL(q, pd)), r0), dd, yy);
-      const float qn = q + (ax ? f0 : (ay ? f1 : f2));
+      const float qn = RFADD(q, 1.0f);
       key += ax ? k0 : (ay ? k1 : k2);
       q0 = ax ? qn : q0;
       q1 = ay ? qn : q1;
@@ -373,7 +381,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total, int* warp
   return before;
 }
 
-template <int H, int T>
+template <int H, int T, bool OISO>
 __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __restrict__ sincos,
                                                     const int32_t* __restrict__ cnl_ids, int64_t row0, int nrays,
                                                     uint32_t seed, const float* __restrict__ rays,
@@ -424,7 +432,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     }
     // start offsets: the thread index bit-reversed, so that neighbouring
     // lanes start far apart along the ray
-    walk_ray(g, ch, r, int(__brev(threadIdx.x) >> 24), emit, emit_key, &bad_walk);
+    walk_ray<OISO>(g, ch, r, int(__brev(threadIdx.x) >> 24), emit, emit_key, &bad_walk);
   }
   __syncthreads();
 
@@ -436,7 +444,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     return;
   }
 
-  // Compaction: keep voxels that pass the cylinder test.
+  // Compaction: keep voxels with a positive sum that pass the cylinder test.
   constexpr int PER = H / T;
   int kr[PER];
   float vr[PER];
@@ -446,7 +454,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     int slot = j * T + tid;
     int key = keys[slot];
     float v = vals[slot];
-    bool ok = key >= 0;
+    bool ok = key >= 0 && v > 0.f;
     if (ok) {
       int ix = key / nyz;
       int rem = key - ix * nyz;
@@ -513,10 +521,14 @@ cudaError_t launch_level(const DGeom& g, const float2* d_sincos, const int32_t* 
                          int nrays, uint32_t seed, const float* d_rays, int32_t* st_col, float* st_val,
                          int32_t* row_nnz, int32_t* d_flags, cudaStream_t s) {
   const size_t smem = size_t(H) * (sizeof(int) + sizeof(float));
-  cudaError_t e = cudaFuncSetAttribute(sm_rows_kernel<H, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  // A grid with the same origin on every axis (the usual centred cube) lets
+  // the walk's step skip selecting the origin.
+  const bool oiso = g.o[0] == g.o[1] && g.o[1] == g.o[2];
+  auto kern = oiso ? sm_rows_kernel<H, T, true> : sm_rows_kernel<H, T, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  sm_rows_kernel<H, T><<<unsigned(nrows), T, smem, s>>>(g, d_sincos, d_cnl, row0, nrays, seed, d_rays, st_col,
-                                                         st_val, row_nnz, d_flags);
+  kern<<<unsigned(nrows), T, smem, s>>>(g, d_sincos, d_cnl, row0, nrays, seed, d_rays, st_col, st_val, row_nnz,
+                                        d_flags);
   note_launches(1);
   return cudaGetLastError();
 }

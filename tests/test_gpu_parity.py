@@ -173,6 +173,20 @@ def test_sysmat_fine_geometry(rlib, oracle):
     assert_rows_equal(*A.to_numpy(), *oracle.sysmat(g, lst, 1000, SEED, method=1))
 
 
+def test_sysmat_anisotropic_offset_grid(rlib, oracle):
+    # Origin, pitch and size differ per axis and the grid is off centre: the
+    # walk's general step (origin selected per axis) against the oracle.
+    g = cfg.Geometry(grid_o=(-0.061, -0.047, -0.039), grid_d=(0.002, 0.0025, 0.0018), grid_n=(60, 40, 48),
+                     pos0x=-0.240, pos1x=0.240, na=12, n0z=13, n0y=13, n1z=13, n1y=13, da=15.0, segx=0.020,
+                     segy=0.004, segz=0.004)
+    ctx = rlib.Context(g, 0)
+    rng = np.random.Generator(np.random.PCG64(10))
+    lst = rng.integers(0, g.n_channels, 80).astype(np.int32)
+    A = ctx.build(lst, 300, SEED)
+    assert A.nnz > 0
+    assert_rows_equal(*A.to_numpy(), *oracle.sysmat(g, lst, 300, SEED, method=1))
+
+
 def test_sysmat_given_rays_with_axis_parallel_rays(rlib, oracle, torch, ctx_small):
     # Identical caller-supplied endpoints, including rays parallel to a plane
     # family, against the reference algorithm (method 0).
