@@ -88,14 +88,70 @@ struct RowTable {
   }
 };
 
+// Where the step walk adds a voxel's length.  KeyIndex tracks the voxel id
+// and adds to the row's hash table; DenseIndex tracks the voxel's slot in
+// the row's slab windows (below) and adds to it directly.  begin() takes the
+// ray's step directions, set() places the index at a voxel, advance() moves
+// it one voxel along the axis the walk steps (x if ax, else y if ay, else z).
+template <int H>
+struct KeyIndex {
+  const RowTable<H>* table;
+  int nyz, nz;
+  int key, k0, k1, k2;
+  __device__ __forceinline__ void begin(const int step[3]) {
+    k0 = step[0] * nyz;
+    k1 = step[1] * nz;
+    k2 = step[2];
+  }
+  __device__ __forceinline__ void set(int i0, int i1, int i2) { key = i0 * nyz + i1 * nz + i2; }
+  __device__ __forceinline__ void advance(bool ax, bool ay) { key += ax ? k0 : (ay ? k1 : k2); }
+  __device__ __forceinline__ void add(float L) const { table->add(key, L); }
+};
+
+// Slab windows of a row whose rays all cross the grid in +x or all in -x:
+// for every x slab s the rays' voxels lie in the y-z window
+// [ylo[s], ylo[s]+wy) x [zlo[s], zlo[s]+wz), which holds wy*wz dense slots
+// from slot s*wy*wz on (slot = base[s] + iy*wz + iz).  A step in y moves the
+// slot by +-wz, in z by +-1, in x by dk[s] (the base difference to the next
+// slab in the rays' x direction).  No key is stored or compared.
+struct DenseIndex {
+  float* acc;
+  const int* base;
+  const int* dk;
+  int wz, nslots;
+  int* fail;
+  int slot, sx, kx, st0, k1, k2;
+  __device__ __forceinline__ void begin(const int step[3]) {
+    st0 = step[0];
+    k1 = step[1] * wz;
+    k2 = step[2];
+  }
+  __device__ __forceinline__ void set(int i0, int i1, int i2) {
+    slot = base[i0] + i1 * wz + i2;
+    sx = i0;
+    kx = dk[i0];
+  }
+  __device__ __forceinline__ void advance(bool ax, bool ay) {
+    slot += ax ? kx : (ay ? k1 : k2);
+    sx = ax ? sx + st0 : sx;
+    kx = dk[sx];
+  }
+  __device__ __forceinline__ void add(float L) const {
+    if (unsigned(slot) < unsigned(nslots))
+      atomicAdd(&acc[slot], L);
+    else
+      *fail = 1;
+  }
+};
+
 // Visits every grid voxel whose intersection length with ray r is positive.
 // emit(ix, iy, iz, L) for the common case of a ray that crosses the planes
 // of all three axes; a ray parallel to the planes of some axis (start and
 // end coordinate equal) leaves that axis unconstrained, as the reference's
 // masked min/max does, and every candidate voxel along it gets the length.
-template <bool OISO, class Emit, class EmitKey>
+template <bool OISO, class Emit, class Index>
 __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, const float r[6], int part, Emit& emit,
-                                         EmitKey& emit_key, int* bad_walk) {
+                                         Index& ix, int* bad_walk) {
   float dir[3];
   bool s[3];
 #pragma unroll
@@ -161,7 +217,14 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
   }
   const bool all3 = s[0] && s[1] && s[2];
   const int guard_max = g.n[0] + g.n[1] + g.n[2] + 8;
-  if (all3) {
+  // The step loop computes plane parameters exactly as plane_alpha_r did
+  // for the grid's bounding planes (same operations and reciprocals), which
+  // keeps every step inside the grid; a direction component outside the
+  // range where plane_alpha_r uses the reciprocal goes to the general loop.
+  bool in_range = true;
+#pragma unroll
+  for (int d = 0; d < 3; d++) in_range = in_range && fabsf(dir[d]) >= 1e-30f && fabsf(dir[d]) <= 1e30f;
+  if (all3 && in_range) {
     // One axis per step, chosen with selects (no runtime array index):
     // the axis whose next plane comes first.  Planes of two axes at the same
     // parameter take two steps; the voxel between them has zero length (its
@@ -170,9 +233,8 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
     float lo0 = lo[0], lo1 = lo[1], lo2 = lo[2];
     float hi0 = hi[0], hi1 = hi[1], hi2 = hi[2];
     const float y0 = rc[0], y1 = rc[1], y2 = rc[2];
-    const int nyz = g.n[1] * g.n[2];
-    int key = i0 * nyz + i1 * g.n[2] + i2;
-    const int k0 = step[0] * nyz, k1 = step[1] * g.n[2], k2 = step[2];
+    ix.begin(step);
+    ix.set(i0, i1, i2);
     // Staggered start: the walk begins at a plane of the dominant axis D,
     // part/256 of the way along the ray, runs to the exit, then wraps
     // around to the entry and runs up to that plane.  No voxel straddles a
@@ -180,7 +242,8 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
     // lengths, while the threads of a row -- nearly parallel rays of one
     // channel -- sit on different voxels at any step instead of adding to
     // the same shared-memory accumulator at once.
-    const int s0 = i0, s1 = i1, s2 = i2, skey = key;
+    const int s0 = i0, s1 = i1, s2 = i2;
+    const Index six = ix;
     const float sl0 = lo0, sl1 = lo1, sl2 = lo2, sh0 = hi0, sh1 = hi1, sh2 = hi2;
     float stop = amax_g, a_split = amax_g;
     bool wrapped = true;
@@ -247,7 +310,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
             hi0 = nh[0];
             hi1 = nh[1];
             hi2 = nh[2];
-            key = i0 * nyz + i1 * g.n[2] + i2;
+            ix.set(i0, i1, i2);
             a_split = as;
             wrapped = false;
           }
@@ -277,7 +340,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
       // A voxel between two planes at the same parameter gets length 0; it
       // is added all the same (no branch) and dropped with the other
       // zero sums when the row is compacted.
-      emit_key(key, RFMUL(RFSUB(a_hi, prev), len));
+      ix.add(RFMUL(RFSUB(a_hi, prev), len));
       // The next plane lies before the exit, so it is not the grid's last
       // plane of its axis, and the step stays inside the grid.
       if (!(a_hi < stop)) {
@@ -289,7 +352,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
         hi0 = sh0;
         hi1 = sh1;
         hi2 = sh2;
-        key = skey;
+        ix = six;
         prev = sprev;
         stop = a_split;
         wrapped = true;
@@ -305,7 +368,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
       const float yy = ax ? y0 : (ay ? y1 : y2);
       const float hn = div_rcp(RFSUB(RFADD(o, RFMUL(q, pd)), r0), dd, yy);
       const float qn = RFADD(q, 1.0f);
-      key += ax ? k0 : (ay ? k1 : k2);
+      ix.advance(ax, ay);
       q0 = ax ? qn : q0;
       q1 = ay ? qn : q1;
       q2 = (!ax && !ay) ? qn : q2;
@@ -381,6 +444,67 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total, int* warp
   return before;
 }
 
+constexpr int kMaxSlabs = 256;
+
+// Row-level decision for the slab windows: both crystals' boxes (corner
+// AABBs) lie on opposite sides of the grid in x, so every ray of the row
+// crosses the whole grid in the same x direction (xdir) and lies in the
+// convex hull of the two boxes.
+__device__ inline void crystal_boxes(const Channel& ch, float lo[2][3], float hi[2][3]) {
+  for (int b = 0; b < 2; b++) {
+    const float* m = b == 0 ? ch.m0 : ch.m1;
+    for (int d = 0; d < 3; d++) {
+      lo[b][d] = INFINITY;
+      hi[b][d] = -INFINITY;
+    }
+    for (int c = 0; c < 8; c++) {
+      float p[3];
+      trafo_apply(m, float(c & 1), float((c >> 1) & 1), float((c >> 2) & 1), p);
+      for (int d = 0; d < 3; d++) {
+        lo[b][d] = fminf(lo[b][d], p[d]);
+        hi[b][d] = fmaxf(hi[b][d], p[d]);
+      }
+    }
+  }
+}
+
+// The y or z voxel range (w = 1 or 2) that rays from box A (lower x) to box
+// B can reach within the x slab [c0, c1]: a ray point at x = c is
+// (1-t)*p + t*q with p in A, q in B and t between (c - bA)/(bB - bA) and
+// (c - aA)/(aB - aA) ([aA, bA], [aB, bB] the boxes' x ranges), so its w lies
+// between the extremes of the boxes' w bounds at those t, at both slab
+// faces.  One voxel of margin on each side covers rounding.
+__device__ inline void slab_window(const DGeom& g, const float alo[3], const float ahi[3], const float blo[3],
+                                   const float bhi[3], float c0, float c1, int w, int* ilo, int* ihi) {
+  float wlo = INFINITY, whi = -INFINITY;
+#pragma unroll
+  for (int e = 0; e < 2; e++) {
+    const float c = e == 0 ? c0 : c1;
+    const float t1 = (c - ahi[0]) / (bhi[0] - ahi[0]);
+    const float t2 = (c - alo[0]) / (blo[0] - alo[0]);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const float t = k == 0 ? t1 : t2;
+      wlo = fminf(wlo, alo[w] + t * (blo[w] - alo[w]));
+      whi = fmaxf(whi, ahi[w] + t * (bhi[w] - ahi[w]));
+    }
+  }
+  const int n = g.n[w];
+  int a = int(floorf((wlo - g.o[w]) / g.d[w])) - 1;
+  int b = int(floorf((whi - g.o[w]) / g.d[w])) + 1;
+  a = min(max(a, 0), n - 1);
+  b = min(max(b, 0), n - 1);
+  *ilo = a;
+  *ihi = max(a, b);
+}
+
+// One CTA per row (channel): its rays are walked by the CTA's threads and
+// their lengths summed per voxel in shared memory, then the voxels that pass
+// the cylinder test are written in column order to the row's staging slot.
+// The sums go to dense slab windows when the row allows it (generated rays,
+// crystals on opposite x sides of the grid, windows within 2H slots), else to
+// an open-addressing hash table of H keys; a dense row that finds a voxel
+// outside its windows is redone with the table.
 template <int H, int T, bool OISO>
 __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __restrict__ sincos,
                                                     const int32_t* __restrict__ cnl_ids, int64_t row0, int nrays,
@@ -390,9 +514,12 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
   extern __shared__ __align__(16) unsigned char smem[];
   int* keys = reinterpret_cast<int*>(smem);
   float* vals = reinterpret_cast<float*>(smem + H * sizeof(int));
+  float* acc = reinterpret_cast<float*>(smem);  // dense mode: 2H slots over both arrays
   __shared__ Channel ch;
-  __shared__ int overflow, bad_walk;
+  __shared__ int overflow, bad_walk, dense, dense_fail, win_y, win_z, xdir;
+  __shared__ float box_lo[2][3], box_hi[2][3];
   __shared__ int warp_sums[32];
+  __shared__ int ylo[kMaxSlabs], zlo[kMaxSlabs], sbase[kMaxSlabs], sdk[kMaxSlabs];
 
   const int tid = threadIdx.x;
   const int64_t li = row0 + blockIdx.x;
@@ -405,42 +532,188 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     return;
   }
 
-  for (int i = tid; i < H; i += T) {
-    keys[i] = -1;
-    vals[i] = 0.f;
-  }
+  const int nyz = g.n[1] * g.n[2];
+  const int nz = g.n[2];
+  const int nx = g.n[0];
   if (tid == 0) {
     channel_setup(g, sincos, cnl, ch);
     overflow = 0;
     bad_walk = 0;
+    dense_fail = 0;
+    win_y = 0;
+    win_z = 0;
+    int ok = 0, dir = 0;
+    if (!rays && nx <= kMaxSlabs) {
+      crystal_boxes(ch, box_lo, box_hi);
+      const float gx0 = g.o[0], gx1 = g.o[0] + float(nx) * g.d[0];
+      const float m = 1e-6f * (1.0f + fabsf(gx0) + fabsf(gx1));
+      if (box_hi[0][0] + m < gx0 && box_lo[1][0] - m > gx1) dir = 1;
+      if (box_hi[1][0] + m < gx0 && box_lo[0][0] - m > gx1) dir = -1;
+      ok = dir != 0;
+    }
+    dense = ok;
+    xdir = dir;
   }
   __syncthreads();
 
-  RowTable<H> table{keys, vals, &overflow};
-  const int nyz = g.n[1] * g.n[2];
-  const int nz = g.n[2];
-  auto emit = [&](int ix, int iy, int iz, float L) { table.add(ix * nyz + iy * nz + iz, L); };
-  auto emit_key = [&](int key, float L) { table.add(key, L); };
-  for (int ray = tid; ray < nrays; ray += T) {
-    float r[6];
-    if (rays) {
-      const float* src = rays + (li * int64_t(nrays) + ray) * 6;
-#pragma unroll
-      for (int k = 0; k < 6; k++) r[k] = src[k];
-    } else {
-      make_ray(ch, seed, cnl, ray, r);
+  if (dense) {
+    const int a = xdir > 0 ? 0 : 1;  // the box at lower x
+    for (int sl = tid; sl < nx; sl += T) {
+      const float c0 = g.o[0] + float(sl) * g.d[0], c1 = g.o[0] + float(sl + 1) * g.d[0];
+      int y0, y1, z0, z1;
+      slab_window(g, box_lo[a], box_hi[a], box_lo[1 - a], box_hi[1 - a], c0, c1, 1, &y0, &y1);
+      slab_window(g, box_lo[a], box_hi[a], box_lo[1 - a], box_hi[1 - a], c0, c1, 2, &z0, &z1);
+      ylo[sl] = y0;
+      zlo[sl] = z0;
+      atomicMax(&win_y, y1 - y0 + 1);
+      atomicMax(&win_z, z1 - z0 + 1);
     }
-    // start offsets: the thread index bit-reversed, so that neighbouring
-    // lanes start far apart along the ray
-    walk_ray<OISO>(g, ch, r, int(__brev(threadIdx.x) >> 24), emit, emit_key, &bad_walk);
+    __syncthreads();
   }
-  __syncthreads();
+  const int wy = win_y, wz = win_z;
+  const int wyz = wy * wz;
+  bool use_dense = dense && (long long)nx * wyz <= 2LL * H;
+  const int nslots = use_dense ? nx * wyz : 0;
+
+  const float fr = float(nrays);
+  const size_t base = size_t(blockIdx.x) * H;
+  // Dense compaction layout: each warp takes a contiguous run of slots
+  // (slab-major, then y, then z: column order).
+  constexpr int NW = T / 32;
+  const int lane = tid & 31, w = tid >> 5;
+  const int seg = ((nslots + NW - 1) / NW + 31) & ~31;
+  const int b0 = min(w * seg, nslots), b1 = min(b0 + seg, nslots);
+  auto voxel = [&](int slot, int* x, int* y, int* z) {
+    const int sx = slot / wyz;
+    const int rem = slot - sx * wyz;
+    const int u = rem / wz;
+    *x = sx;
+    *y = ylo[sx] + u;
+    *z = zlo[sx] + (rem - u * wz);
+  };
+  for (int pass = 0; pass < 2; pass++) {
+    if (use_dense) {
+      for (int sl = tid; sl < nx; sl += T) {
+        const int b = sl * wyz - ylo[sl] * wz - zlo[sl];
+        const int nb = xdir > 0 ? sl + 1 : sl - 1;
+        const int bn = (nb >= 0 && nb < nx) ? nb * wyz - ylo[nb] * wz - zlo[nb] : b;
+        sbase[sl] = b;
+        sdk[sl] = bn - b;
+      }
+      for (int i = tid; i < nslots; i += T) acc[i] = 0.f;
+    } else {
+      for (int i = tid; i < H; i += T) {
+        keys[i] = -1;
+        vals[i] = 0.f;
+      }
+    }
+    __syncthreads();
+
+    if (use_dense) {
+      DenseIndex dix{acc, sbase, sdk, wz, nslots, &dense_fail};
+      auto emit = [&](int ix, int iy, int iz, float L) {
+        const int u = iy - ylo[ix], v = iz - zlo[ix];
+        if (unsigned(u) < unsigned(wy) && unsigned(v) < unsigned(wz))
+          atomicAdd(&acc[ix * wyz + u * wz + v], L);
+        else
+          dense_fail = 1;
+      };
+      for (int ray = tid; ray < nrays; ray += T) {
+        float r[6];
+        make_ray(ch, seed, cnl, ray, r);
+        const float dx = RFSUB(r[3], r[0]);
+        if (xdir > 0 ? !(dx > 0.f) : !(dx < 0.f)) dense_fail = 1;
+        // start offsets: the thread index bit-reversed, so that neighbouring
+        // lanes start far apart along the ray
+        walk_ray<OISO>(g, ch, r, int(__brev(threadIdx.x) >> 24), emit, dix, &bad_walk);
+      }
+    } else {
+      RowTable<H> table{keys, vals, &overflow};
+      KeyIndex<H> kix{&table, nyz, nz};
+      auto emit = [&](int ix, int iy, int iz, float L) { table.add(ix * nyz + iy * nz + iz, L); };
+      for (int ray = tid; ray < nrays; ray += T) {
+        float r[6];
+        if (rays) {
+          const float* src = rays + (li * int64_t(nrays) + ray) * 6;
+#pragma unroll
+          for (int k = 0; k < 6; k++) r[k] = src[k];
+        } else {
+          make_ray(ch, seed, cnl, ray, r);
+        }
+        walk_ray<OISO>(g, ch, r, int(__brev(threadIdx.x) >> 24), emit, kix, &bad_walk);
+      }
+    }
+    __syncthreads();
+    if (use_dense && !dense_fail && !bad_walk) {
+      // First compaction pass: per warp, count the voxels with a positive
+      // sum that pass the cylinder test and clear the others.  A positive
+      // slot that decodes to a voxel outside the grid means the windows
+      // missed a voxel: the row is redone with the table.
+      int cnt = 0;
+      for (int b = b0; b < b1; b += 32) {
+        const int slot = b + lane;
+        bool keep = false;
+        if (slot < b1) {
+          const float v = acc[slot];
+          if (v > 0.f) {
+            int x, y, z;
+            voxel(slot, &x, &y, &z);
+            if (y < g.n[1] && z < g.n[2]) {
+              keep = candidate_test(g, ch, x, y, z);
+            } else {
+              dense_fail = 1;
+            }
+            if (!keep) acc[slot] = 0.f;
+          }
+        }
+        cnt += __popc(__ballot_sync(0xffffffffu, keep));
+      }
+      if (lane == 0) warp_sums[w] = cnt;
+      __syncthreads();
+    }
+    if (!(use_dense && dense_fail)) break;
+    use_dense = false;  // redo the row with the table
+    __syncthreads();
+  }
 
   if (overflow || bad_walk) {
     if (tid == 0) {
       row_nnz[blockIdx.x] = -1;
       atomicOr(flags, overflow ? 1 : 2);
     }
+    return;
+  }
+
+  if (use_dense) {
+    // Second pass: after a scan of the warp counts, each warp writes its
+    // voxels in slot order.
+    int before = 0, total = 0;
+    for (int k = 0; k < NW; k++) {
+      const int c = warp_sums[k];
+      before += k < w ? c : 0;
+      total += c;
+    }
+    if (total > H) {
+      if (tid == 0) {
+        row_nnz[blockIdx.x] = -1;
+        atomicOr(flags, 1);
+      }
+      return;
+    }
+    for (int b = b0; b < b1; b += 32) {
+      const int slot = b + lane;
+      const bool keep = slot < b1 && acc[slot] > 0.f;
+      const unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int pos = before + __popc(m & ((1u << lane) - 1u));
+        int x, y, z;
+        voxel(slot, &x, &y, &z);
+        st_col[base + pos] = x * nyz + y * nz + z;
+        st_val[base + pos] = RFDIV(acc[slot], fr);
+      }
+      before += __popc(m);
+    }
+    if (tid == 0) row_nnz[blockIdx.x] = total;
     return;
   }
 
@@ -501,8 +774,6 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     }
   }
 
-  const size_t base = size_t(blockIdx.x) * H;
-  const float fr = float(nrays);
   for (int i = tid; i < total; i += T) {
     st_col[base + i] = keys[i];
     st_val[base + i] = RFDIV(vals[i], fr);
