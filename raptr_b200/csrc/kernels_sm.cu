@@ -108,33 +108,40 @@ struct KeyIndex {
   __device__ __forceinline__ void add(float L) const { table->add(key, L); }
 };
 
-// Slab windows of a row whose rays all cross the grid in +x or all in -x:
-// for every x slab s the rays' voxels lie in the y-z window
-// [ylo[s], ylo[s]+wy) x [zlo[s], zlo[s]+wz), which holds wy*wz dense slots
-// from slot s*wy*wz on (slot = base[s] + iy*wz + iz).  A step in y moves the
-// slot by +-wz, in z by +-1, in x by dk[s] (the base difference to the next
-// slab in the rays' x direction).  No key is stored or compared.
+// Slab windows of a row whose rays all cross the grid in the same direction
+// along the slab axis A (x or z): for every slab s of A the rays' voxels lie
+// in a window [ulo[s], ulo[s]+wu) x [vlo[s], vlo[s]+wv) of the other two
+// axes U < V (y, z for A = x; x, y for A = z), which holds wu*wv dense slots
+// from slot s*wu*wv on (slot = base[s] + iu*wv + iv).  A step in U moves the
+// slot by +-wv, in V by +-1, in A by dk[s] (the base difference to the next
+// slab in the rays' direction).  No key is stored or compared.
+template <int A>
 struct DenseIndex {
   float* acc;
   const int* base;
   const int* dk;
-  int wz, nslots;
+  int wv, nslots;
   int* fail;
-  int slot, sx, kx, st0, k1, k2;
+  int slot, sa, ka, sta, ku, kv;
   __device__ __forceinline__ void begin(const int step[3]) {
-    st0 = step[0];
-    k1 = step[1] * wz;
-    k2 = step[2];
+    sta = step[A];
+    ku = step[A == 0 ? 1 : 0] * wv;
+    kv = step[A == 0 ? 2 : 1];
   }
   __device__ __forceinline__ void set(int i0, int i1, int i2) {
-    slot = base[i0] + i1 * wz + i2;
-    sx = i0;
-    kx = dk[i0];
+    sa = A == 0 ? i0 : i2;
+    slot = A == 0 ? base[i0] + i1 * wv + i2 : base[i2] + i0 * wv + i1;
+    ka = dk[sa];
   }
   __device__ __forceinline__ void advance(bool ax, bool ay) {
-    slot += ax ? kx : (ay ? k1 : k2);
-    sx = ax ? sx + st0 : sx;
-    kx = dk[sx];
+    if (A == 0) {
+      slot += ax ? ka : (ay ? ku : kv);
+      sa = ax ? sa + sta : sa;
+    } else {
+      slot += ax ? ku : (ay ? kv : ka);
+      sa = (ax || ay) ? sa : sa + sta;
+    }
+    ka = dk[sa];
   }
   __device__ __forceinline__ void add(float L) const {
     if (unsigned(slot) < unsigned(nslots))
@@ -468,43 +475,45 @@ __device__ inline void crystal_boxes(const Channel& ch, float lo[2][3], float hi
   }
 }
 
-// The y or z voxel range (w = 1 or 2) that rays from box A (lower x) to box
-// B can reach within the x slab [c0, c1]: a ray point at x = c is
-// (1-t)*p + t*q with p in A, q in B and t between (c - bA)/(bB - bA) and
-// (c - aA)/(aB - aA) ([aA, bA], [aB, bB] the boxes' x ranges), so its w lies
-// between the extremes of the boxes' w bounds at those t, at both slab
-// faces.  One voxel of margin on each side covers rounding.
-__device__ inline void slab_window(const DGeom& g, const float alo[3], const float ahi[3], const float blo[3],
-                                   const float bhi[3], float c0, float c1, int w, int* ilo, int* ihi) {
+// The voxel range along axis w that rays from box P (lower coordinate on
+// the slab axis a) to box Q can reach within the slab [c0, c1] of axis a: a
+// ray point at coordinate c is (1-t)*p + t*q with p in P, q in Q and t
+// between (c - bP)/(bQ - bP) and (c - aP)/(aQ - aP) ([aP, bP], [aQ, bQ] the
+// boxes' ranges along a), so its w lies between the extremes of the boxes'
+// w bounds at those t, at both slab faces.  One voxel of margin on each
+// side covers rounding.
+__device__ inline void slab_window(const DGeom& g, int a, const float plo[3], const float phi[3],
+                                   const float qlo[3], const float qhi[3], float c0, float c1, int w, int* ilo,
+                                   int* ihi) {
   float wlo = INFINITY, whi = -INFINITY;
 #pragma unroll
   for (int e = 0; e < 2; e++) {
     const float c = e == 0 ? c0 : c1;
-    const float t1 = (c - ahi[0]) / (bhi[0] - ahi[0]);
-    const float t2 = (c - alo[0]) / (blo[0] - alo[0]);
+    const float t1 = (c - phi[a]) / (qhi[a] - phi[a]);
+    const float t2 = (c - plo[a]) / (qlo[a] - plo[a]);
 #pragma unroll
     for (int k = 0; k < 2; k++) {
       const float t = k == 0 ? t1 : t2;
-      wlo = fminf(wlo, alo[w] + t * (blo[w] - alo[w]));
-      whi = fmaxf(whi, ahi[w] + t * (bhi[w] - ahi[w]));
+      wlo = fminf(wlo, plo[w] + t * (qlo[w] - plo[w]));
+      whi = fmaxf(whi, phi[w] + t * (qhi[w] - phi[w]));
     }
   }
   const int n = g.n[w];
-  int a = int(floorf((wlo - g.o[w]) / g.d[w])) - 1;
-  int b = int(floorf((whi - g.o[w]) / g.d[w])) + 1;
-  a = min(max(a, 0), n - 1);
-  b = min(max(b, 0), n - 1);
-  *ilo = a;
-  *ihi = max(a, b);
+  int lo = int(floorf((wlo - g.o[w]) / g.d[w])) - 1;
+  int hi = int(floorf((whi - g.o[w]) / g.d[w])) + 1;
+  lo = min(max(lo, 0), n - 1);
+  hi = min(max(hi, 0), n - 1);
+  *ilo = lo;
+  *ihi = max(lo, hi);
 }
 
 // One CTA per row (channel): its rays are walked by the CTA's threads and
 // their lengths summed per voxel in shared memory, then the voxels that pass
 // the cylinder test are written in column order to the row's staging slot.
 // The sums go to dense slab windows when the row allows it (generated rays,
-// crystals on opposite x sides of the grid, windows within 2H slots), else to
-// an open-addressing hash table of H keys; a dense row that finds a voxel
-// outside its windows is redone with the table.
+// crystals on opposite sides of the grid along x or z, windows within 2H
+// slots), else to an open-addressing hash table of H keys; a dense row that
+// finds a voxel outside its windows is redone with the table.
 template <int H, int T, bool OISO>
 __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __restrict__ sincos,
                                                     const int32_t* __restrict__ cnl_ids, int64_t row0, int nrays,
@@ -516,10 +525,10 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
   float* vals = reinterpret_cast<float*>(smem + H * sizeof(int));
   float* acc = reinterpret_cast<float*>(smem);  // dense mode: 2H slots over both arrays
   __shared__ Channel ch;
-  __shared__ int overflow, bad_walk, dense, dense_fail, win_y, win_z, xdir;
+  __shared__ int overflow, bad_walk, dense_fail, win_u, win_v, sax, sdir;
   __shared__ float box_lo[2][3], box_hi[2][3];
   __shared__ int warp_sums[32];
-  __shared__ int ylo[kMaxSlabs], zlo[kMaxSlabs], sbase[kMaxSlabs], sdk[kMaxSlabs];
+  __shared__ int ulo[kMaxSlabs], vlo[kMaxSlabs], sbase[kMaxSlabs], sdk[kMaxSlabs];
 
   const int tid = threadIdx.x;
   const int64_t li = row0 + blockIdx.x;
@@ -534,69 +543,77 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
 
   const int nyz = g.n[1] * g.n[2];
   const int nz = g.n[2];
-  const int nx = g.n[0];
   if (tid == 0) {
     channel_setup(g, sincos, cnl, ch);
     overflow = 0;
     bad_walk = 0;
     dense_fail = 0;
-    win_y = 0;
-    win_z = 0;
-    int ok = 0, dir = 0;
-    if (!rays && nx <= kMaxSlabs) {
+    win_u = 0;
+    win_v = 0;
+    int axis = -1, dir = 0;
+    if (!rays) {
       crystal_boxes(ch, box_lo, box_hi);
-      const float gx0 = g.o[0], gx1 = g.o[0] + float(nx) * g.d[0];
-      const float m = 1e-6f * (1.0f + fabsf(gx0) + fabsf(gx1));
-      if (box_hi[0][0] + m < gx0 && box_lo[1][0] - m > gx1) dir = 1;
-      if (box_hi[1][0] + m < gx0 && box_lo[0][0] - m > gx1) dir = -1;
-      ok = dir != 0;
+      // the slab axis: x if the crystals lie on opposite x sides of the
+      // grid, else z if they do along z
+      for (int a = 0; a <= 2 && axis < 0; a += 2) {
+        if (g.n[a] > kMaxSlabs) continue;
+        const float c0 = g.o[a], c1 = g.o[a] + float(g.n[a]) * g.d[a];
+        const float m = 1e-6f * (1.0f + fabsf(c0) + fabsf(c1));
+        if (box_hi[0][a] + m < c0 && box_lo[1][a] - m > c1) dir = 1;
+        if (box_hi[1][a] + m < c0 && box_lo[0][a] - m > c1) dir = -1;
+        if (dir != 0) axis = a;
+      }
     }
-    dense = ok;
-    xdir = dir;
+    sax = axis;
+    sdir = dir;
   }
   __syncthreads();
 
-  if (dense) {
-    const int a = xdir > 0 ? 0 : 1;  // the box at lower x
-    for (int sl = tid; sl < nx; sl += T) {
-      const float c0 = g.o[0] + float(sl) * g.d[0], c1 = g.o[0] + float(sl + 1) * g.d[0];
-      int y0, y1, z0, z1;
-      slab_window(g, box_lo[a], box_hi[a], box_lo[1 - a], box_hi[1 - a], c0, c1, 1, &y0, &y1);
-      slab_window(g, box_lo[a], box_hi[a], box_lo[1 - a], box_hi[1 - a], c0, c1, 2, &z0, &z1);
-      ylo[sl] = y0;
-      zlo[sl] = z0;
-      atomicMax(&win_y, y1 - y0 + 1);
-      atomicMax(&win_z, z1 - z0 + 1);
+  const int A = sax;
+  const int iu_ax = A == 0 ? 1 : 0, iv_ax = A == 0 ? 2 : 1;
+  const int na = A >= 0 ? g.n[A] : 0;
+  if (A >= 0) {
+    const int p = sdir > 0 ? 0 : 1;  // the box at the lower coordinate along A
+    for (int sl = tid; sl < na; sl += T) {
+      const float c0 = g.o[A] + float(sl) * g.d[A], c1 = g.o[A] + float(sl + 1) * g.d[A];
+      int u0, u1, v0, v1;
+      slab_window(g, A, box_lo[p], box_hi[p], box_lo[1 - p], box_hi[1 - p], c0, c1, iu_ax, &u0, &u1);
+      slab_window(g, A, box_lo[p], box_hi[p], box_lo[1 - p], box_hi[1 - p], c0, c1, iv_ax, &v0, &v1);
+      ulo[sl] = u0;
+      vlo[sl] = v0;
+      atomicMax(&win_u, u1 - u0 + 1);
+      atomicMax(&win_v, v1 - v0 + 1);
     }
     __syncthreads();
   }
-  const int wy = win_y, wz = win_z;
-  const int wyz = wy * wz;
-  bool use_dense = dense && (long long)nx * wyz <= 2LL * H;
-  const int nslots = use_dense ? nx * wyz : 0;
+  const int wu = win_u, wv = win_v;
+  const int wuv = wu * wv;
+  bool use_dense = A >= 0 && (long long)na * wuv <= 2LL * H;
+  const int nslots = use_dense ? na * wuv : 0;
 
   const float fr = float(nrays);
   const size_t base = size_t(blockIdx.x) * H;
   // Dense compaction layout: each warp takes a contiguous run of slots
-  // (slab-major, then y, then z: column order).
+  // (slab-major, then U, then V).
   constexpr int NW = T / 32;
   const int lane = tid & 31, w = tid >> 5;
   const int seg = ((nslots + NW - 1) / NW + 31) & ~31;
   const int b0 = min(w * seg, nslots), b1 = min(b0 + seg, nslots);
   auto voxel = [&](int slot, int* x, int* y, int* z) {
-    const int sx = slot / wyz;
-    const int rem = slot - sx * wyz;
-    const int u = rem / wz;
-    *x = sx;
-    *y = ylo[sx] + u;
-    *z = zlo[sx] + (rem - u * wz);
+    const int sa = slot / wuv;
+    const int rem = slot - sa * wuv;
+    const int u = rem / wv;
+    const int iu = ulo[sa] + u, iv = vlo[sa] + (rem - u * wv);
+    *x = A == 0 ? sa : iu;
+    *y = A == 0 ? iu : iv;
+    *z = A == 0 ? iv : sa;
   };
   for (int pass = 0; pass < 2; pass++) {
     if (use_dense) {
-      for (int sl = tid; sl < nx; sl += T) {
-        const int b = sl * wyz - ylo[sl] * wz - zlo[sl];
-        const int nb = xdir > 0 ? sl + 1 : sl - 1;
-        const int bn = (nb >= 0 && nb < nx) ? nb * wyz - ylo[nb] * wz - zlo[nb] : b;
+      for (int sl = tid; sl < na; sl += T) {
+        const int b = sl * wuv - ulo[sl] * wv - vlo[sl];
+        const int nb = sdir > 0 ? sl + 1 : sl - 1;
+        const int bn = (nb >= 0 && nb < na) ? nb * wuv - ulo[nb] * wv - vlo[nb] : b;
         sbase[sl] = b;
         sdk[sl] = bn - b;
       }
@@ -610,22 +627,28 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     __syncthreads();
 
     if (use_dense) {
-      DenseIndex dix{acc, sbase, sdk, wz, nslots, &dense_fail};
       auto emit = [&](int ix, int iy, int iz, float L) {
-        const int u = iy - ylo[ix], v = iz - zlo[ix];
-        if (unsigned(u) < unsigned(wy) && unsigned(v) < unsigned(wz))
-          atomicAdd(&acc[ix * wyz + u * wz + v], L);
+        const int sa = A == 0 ? ix : iz;
+        const int u = (A == 0 ? iy : ix) - ulo[sa], v = (A == 0 ? iz : iy) - vlo[sa];
+        if (unsigned(u) < unsigned(wu) && unsigned(v) < unsigned(wv))
+          atomicAdd(&acc[sa * wuv + u * wv + v], L);
         else
           dense_fail = 1;
       };
+      DenseIndex<0> dix0{acc, sbase, sdk, wv, nslots, &dense_fail};
+      DenseIndex<2> dix2{acc, sbase, sdk, wv, nslots, &dense_fail};
       for (int ray = tid; ray < nrays; ray += T) {
         float r[6];
         make_ray(ch, seed, cnl, ray, r);
-        const float dx = RFSUB(r[3], r[0]);
-        if (xdir > 0 ? !(dx > 0.f) : !(dx < 0.f)) dense_fail = 1;
+        const float da = A == 0 ? RFSUB(r[3], r[0]) : RFSUB(r[5], r[2]);
+        if (sdir > 0 ? !(da > 0.f) : !(da < 0.f)) dense_fail = 1;
         // start offsets: the thread index bit-reversed, so that neighbouring
         // lanes start far apart along the ray
-        walk_ray<OISO>(g, ch, r, int(__brev(threadIdx.x) >> 24), emit, dix, &bad_walk);
+        const int part = int(__brev(threadIdx.x) >> 24);
+        if (A == 0)
+          walk_ray<OISO>(g, ch, r, part, emit, dix0, &bad_walk);
+        else
+          walk_ray<OISO>(g, ch, r, part, emit, dix2, &bad_walk);
       }
     } else {
       RowTable<H> table{keys, vals, &overflow};
@@ -658,7 +681,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
           if (v > 0.f) {
             int x, y, z;
             voxel(slot, &x, &y, &z);
-            if (y < g.n[1] && z < g.n[2]) {
+            if (x < g.n[0] && y < g.n[1] && z < g.n[2]) {
               keep = candidate_test(g, ch, x, y, z);
             } else {
               dense_fail = 1;
@@ -684,10 +707,12 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     return;
   }
 
+  int total = 0;
   if (use_dense) {
     // Second pass: after a scan of the warp counts, each warp writes its
-    // voxels in slot order.
-    int before = 0, total = 0;
+    // voxels in slot order -- column order for x slabs; z slabs are sorted
+    // below.
+    int before = 0;
     for (int k = 0; k < NW; k++) {
       const int c = warp_sums[k];
       before += k < w ? c : 0;
@@ -713,40 +738,47 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
       }
       before += __popc(m);
     }
-    if (tid == 0) row_nnz[blockIdx.x] = total;
-    return;
-  }
-
-  // Compaction: keep voxels with a positive sum that pass the cylinder test.
-  constexpr int PER = H / T;
-  int kr[PER];
-  float vr[PER];
-  int cnt = 0;
-#pragma unroll
-  for (int j = 0; j < PER; j++) {
-    int slot = j * T + tid;
-    int key = keys[slot];
-    float v = vals[slot];
-    bool ok = key >= 0 && v > 0.f;
-    if (ok) {
-      int ix = key / nyz;
-      int rem = key - ix * nyz;
-      int iy = rem / nz;
-      int iz = rem - iy * nz;
-      ok = candidate_test(g, ch, ix, iy, iz);
+    if (A == 0) {
+      if (tid == 0) row_nnz[blockIdx.x] = total;
+      return;
     }
-    kr[j] = ok ? key : -1;
-    vr[j] = v;
-    cnt += ok ? 1 : 0;
-  }
-  int total;
-  int pos = block_exclusive_scan<T>(cnt, &total, warp_sums);
+    __syncthreads();
+    for (int i = tid; i < total; i += T) {
+      keys[i] = st_col[base + i];
+      vals[i] = st_val[base + i];
+    }
+  } else {
+    // Compaction: keep voxels with a positive sum that pass the cylinder
+    // test.
+    constexpr int PER = H / T;
+    int kr[PER];
+    float vr[PER];
+    int cnt = 0;
 #pragma unroll
-  for (int j = 0; j < PER; j++) {
-    if (kr[j] >= 0) {
-      keys[pos] = kr[j];
-      vals[pos] = vr[j];
-      pos++;
+    for (int j = 0; j < PER; j++) {
+      int slot = j * T + tid;
+      int key = keys[slot];
+      float v = vals[slot];
+      bool ok = key >= 0 && v > 0.f;
+      if (ok) {
+        int ix = key / nyz;
+        int rem = key - ix * nyz;
+        int iy = rem / nz;
+        int iz = rem - iy * nz;
+        ok = candidate_test(g, ch, ix, iy, iz);
+      }
+      kr[j] = ok ? key : -1;
+      vr[j] = ok ? RFDIV(v, fr) : 0.f;
+      cnt += ok ? 1 : 0;
+    }
+    int pos = block_exclusive_scan<T>(cnt, &total, warp_sums);
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      if (kr[j] >= 0) {
+        keys[pos] = kr[j];
+        vals[pos] = vr[j];
+        pos++;
+      }
     }
   }
   int npad = 1;
@@ -776,7 +808,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
 
   for (int i = tid; i < total; i += T) {
     st_col[base + i] = keys[i];
-    st_val[base + i] = RFDIV(vals[i], fr);
+    st_val[base + i] = vals[i];
   }
   if (tid == 0) row_nnz[blockIdx.x] = total;
 }
