@@ -7,10 +7,14 @@
 // src/MeasurementSetupTrafo2CartCoord.hpp:110-111; it is compiled with
 // -ffp-contract=off so the expression is evaluated as written.
 #include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdlib>
 #include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -30,6 +34,38 @@ raptr_status fail(raptr_status s, const std::string& msg) {
   g_last_error = msg;
   return s;
 }
+
+}  // namespace
+
+namespace raptr {
+
+double trace_ms() {
+  using clk = std::chrono::steady_clock;
+  static const clk::time_point t0 = clk::now();
+  return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+}
+
+bool trace_on() {
+  static const bool on = [] {
+    const char* v = std::getenv("RAPTR_TRACE");
+    return v && *v && std::strcmp(v, "0") != 0;
+  }();
+  return on;
+}
+
+void trace(const char* fmt, ...) {
+  if (!trace_on()) return;
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  std::fprintf(stderr, "[raptr %10.1f ms] %s\n", trace_ms(), buf);
+}
+
+}  // namespace raptr
+
+namespace {
 
 raptr_status cuda_fail(cudaError_t e, const char* what) {
   cudaGetLastError();  // clear a sticky launch error for the next call
@@ -118,6 +154,9 @@ struct raptr_ctx {
   // Small fixed device scratch.
   int64_t* d_i64 = nullptr;   // 64 entries
   int32_t* d_flags = nullptr; // 16 entries
+  // Page-locked host words that asynchronous reads of flags and totals land
+  // in (allocated on first use).
+  int64_t* h_pin = nullptr;   // 16 entries
   double* d_f64 = nullptr;    // 64 entries
   // Voxels in compact (y, z) tubes along x: the column order of the
   // batched back pass, built on first use.
@@ -221,8 +260,13 @@ struct BuildOut {
 raptr_status ensure_capacity(BuildOut& o, int64_t need, int64_t rows_done, cudaStream_t s) {
   if (need <= o.cap || !o.grow) return RAPTR_OK;
   double per_row = rows_done > 0 ? double(need) / double(rows_done) : 0.0;
-  int64_t projected = int64_t(per_row * double(o.n_list) * 1.05) + 1024;
+  // rows of a list differ in length (by projection angle, say): an estimate
+  // from its first quarter gets more headroom, so that the output is not
+  // regrown (a copy of everything so far) near the end
+  const double headroom = rows_done * 4 < o.n_list ? 1.3 : 1.05;
+  int64_t projected = int64_t(per_row * double(o.n_list) * headroom) + 1024;
   int64_t ncap = std::max(need + (need >> 3), projected);
+  const double t0 = trace_on() ? trace_ms() : 0.0;
   int32_t* ncol = nullptr;
   float* nval = nullptr;
   RCU(cudaMalloc(&ncol, size_t(ncap) * sizeof(int32_t)));
@@ -245,6 +289,8 @@ raptr_status ensure_capacity(BuildOut& o, int64_t need, int64_t rows_done, cudaS
   o.grow->col = ncol;
   o.grow->val = nval;
   o.grow->cap = ncap;
+  if (trace_on())
+    trace("build output grown to %lld entries (kept %lld): %.2f ms", (long long)ncap, (long long)keep, trace_ms() - t0);
   return RAPTR_OK;
 }
 
@@ -260,6 +306,144 @@ struct Builder {
   BuildOut& out;
   int64_t total = 0;       // entries placed so far (host mirror of d_base)
   int64_t rows_done = 0;
+
+  // Builds rows [row0, row0+nrows) at `level` as a pipeline of chunks: the
+  // row kernel of chunk i+1 runs on the caller's stream while chunk i is
+  // placed (scan, capacity, gather) on a second stream, from a second
+  // staging buffer, so the device does not idle while the host reads a
+  // chunk's flags and entry count.  A chunk whose table overflowed drains
+  // the pipeline, is rebuilt at the next level by rows(), and the pipeline
+  // restarts after it.
+  raptr_status rows_pipelined(int level, int64_t row0, int64_t nrows) {
+    const int H = sm_level_capacity(level);
+    int64_t per = std::max<int64_t>(1, int64_t(kStagingBudget / (size_t(H) * 8)));
+    per = std::min<int64_t>(per, 65536);
+    if (!ctx->h_pin) RCU(cudaMallocHost(&ctx->h_pin, 16 * sizeof(int64_t)));
+    volatile int32_t* h_flags = reinterpret_cast<volatile int32_t*>(ctx->h_pin);  // 2 words
+    volatile int64_t* h_total = ctx->h_pin + 2;
+    cudaStream_t P = nullptr;
+    cudaEvent_t ev_k[2] = {nullptr, nullptr}, ev_g[2] = {nullptr, nullptr}, ev_j = nullptr;
+    auto release = [&]() {
+      for (auto e : ev_k) if (e) cudaEventDestroy(e);
+      for (auto e : ev_g) if (e) cudaEventDestroy(e);
+      if (ev_j) cudaEventDestroy(ev_j);
+      if (P) cudaStreamDestroy(P);
+    };
+    struct Guard {
+      std::function<void()> f;
+      ~Guard() { f(); }
+    } guard{release};
+    RCU(cudaStreamCreateWithFlags(&P, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; b++) {
+      RCU(cudaEventCreateWithFlags(&ev_k[b], cudaEventDisableTiming));
+      RCU(cudaEventCreateWithFlags(&ev_g[b], cudaEventDisableTiming));
+    }
+    RCU(cudaEventCreateWithFlags(&ev_j, cudaEventDisableTiming));
+    auto drain = [&]() -> cudaError_t {
+      cudaError_t e = cudaStreamSynchronize(s);
+      cudaError_t e2 = cudaStreamSynchronize(P);
+      return e != cudaSuccess ? e : e2;
+    };
+    const int64_t end = row0 + nrows;
+    int64_t r0 = row0;
+    while (r0 < end) {
+      const int64_t n = (end - r0 + per - 1) / per;  // chunks from r0 on
+      size_t need = Carve::need({size_t(per) * H * sizeof(int32_t), size_t(per) * H * sizeof(float),
+                                 size_t(per) * sizeof(int32_t), size_t(per) * H * sizeof(int32_t),
+                                 size_t(per) * H * sizeof(float), size_t(per) * sizeof(int32_t)});
+      RCHECK(ctx->ensure_scratch(need));
+      Carve cv(ctx->d_scratch);
+      int32_t* st_col[2];
+      float* st_val[2];
+      int32_t* row_nnz[2];
+      for (int b = 0; b < 2; b++) {
+        st_col[b] = cv.take<int32_t>(size_t(per) * H);
+        st_val[b] = cv.take<float>(size_t(per) * H);
+        row_nnz[b] = cv.take<int32_t>(size_t(per));
+      }
+      // placement starts after the caller's earlier work
+      RCU(cudaEventRecord(ev_j, s));
+      RCU(cudaStreamWaitEvent(P, ev_j, 0));
+      auto launch = [&](int64_t i) -> cudaError_t {
+        const int b = int(i & 1);
+        const int64_t r = r0 + i * per, k = std::min(per, end - r);
+        cudaError_t e = cudaSuccess;
+        if (i >= 2) e = cudaStreamWaitEvent(s, ev_g[b], 0);  // chunk i-2 has left this buffer
+        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_flags + b, 0, sizeof(int32_t), s);
+        if (e == cudaSuccess)
+          e = launch_sm_rows(level, ctx->dg, ctx->d_sincos, d_cnl, r, k, nrays, seed, d_rays, st_col[b], st_val[b],
+                             row_nnz[b], ctx->d_flags + b, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(const_cast<int32_t*>(h_flags) + b, ctx->d_flags + b, sizeof(int32_t),
+                              cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_k[b], s);
+        return e;
+      };
+      cudaError_t e = launch(0);
+      if (e != cudaSuccess) {
+        drain();
+        return cuda_fail(e, "system-matrix rows");
+      }
+      int64_t next_r0 = end;
+      for (int64_t i = 0; i < n; i++) {
+        const int b = int(i & 1);
+        const int64_t r = r0 + i * per, k = std::min(per, end - r);
+        const double t0 = trace_on() ? trace_ms() : 0.0;
+        if (i + 1 < n) e = launch(i + 1);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev_k[b]);
+        if (e != cudaSuccess) {
+          drain();
+          return cuda_fail(e, "system-matrix rows");
+        }
+        const int32_t flags = h_flags[b];
+        if (flags & 6) {
+          RCU(drain());
+          if (flags & 4) return fail(RAPTR_ERR_INVALID, "a channel id is outside [0, number of channels)");
+          return fail(RAPTR_ERR_OVERFLOW, "ray walk did not terminate (internal error)");
+        }
+        if (flags & 1) {
+          RCU(drain());
+          if (level + 1 >= sm_num_levels())
+            return fail(RAPTR_ERR_OVERFLOW, "a row has more distinct voxels than the largest per-row table holds");
+          RCHECK(rows(level + 1, r, k));
+          next_r0 = r + k;
+          break;
+        }
+        e = cudaStreamWaitEvent(P, ev_k[b], 0);
+        if (e == cudaSuccess) e = launch_rows_scan(row_nnz[b], k, out.rp + r, ctx->d_i64, P);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(const_cast<int64_t*>(h_total), ctx->d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, P);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(P);
+        if (e != cudaSuccess) {
+          drain();
+          return cuda_fail(e, "system-matrix placement");
+        }
+        const int64_t new_total = *h_total;
+        rows_done += k;
+        if (trace_on())
+          trace("build rows %lld+%lld level %d: rows and placement %.2f ms, %lld entries", (long long)r,
+                (long long)k, level, trace_ms() - t0, (long long)new_total);
+        raptr_status st = ensure_capacity(out, new_total, rows_done, P);
+        if (st != RAPTR_OK) {
+          drain();
+          return st;
+        }
+        e = launch_rows_gather(st_col[b], st_val[b], H, out.rp + r, k, out.cap, out.col, out.val, P);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_g[b], P);
+        if (e != cudaSuccess) {
+          drain();
+          return cuda_fail(e, "system-matrix placement");
+        }
+        total = new_total;
+      }
+      // the caller's stream continues after the placement
+      RCU(cudaEventRecord(ev_j, P));
+      RCU(cudaStreamWaitEvent(s, ev_j, 0));
+      if (next_r0 < end) RCU(drain());  // buffers are re-carved after rows() used the scratch
+      r0 = next_r0;
+    }
+    return RAPTR_OK;
+  }
 
   // Builds rows [row0, row0+nrows) at `level`, retrying at higher levels on
   // table overflow, and places them.
@@ -279,6 +463,7 @@ struct Builder {
       int32_t* row_nnz = cv.take<int32_t>(size_t(k));
       int64_t* cand = cv.take<int64_t>(size_t(k));
       (void)cand;
+      const double t0 = trace_on() ? trace_ms() : 0.0;
       RCU(cudaMemsetAsync(ctx->d_flags, 0, sizeof(int32_t), s));
       RCU(launch_sm_rows(level, ctx->dg, ctx->d_sincos, d_cnl, r, k, nrays, seed, d_rays, st_col, st_val, row_nnz,
                          ctx->d_flags, s));
@@ -305,6 +490,9 @@ struct Builder {
       RCU(cudaMemcpyAsync(&new_total, ctx->d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
       RCU(cudaStreamSynchronize(s));
       rows_done += k;
+      if (trace_on())
+        trace("build rows %lld+%lld level %d: rows and placement %.2f ms, %lld entries", (long long)r, (long long)k,
+              level, trace_ms() - t0, (long long)new_total);
       RCHECK(ensure_capacity(out, new_total, rows_done, s));
       if (!keep_zeros) {
         RCU(launch_rows_gather(st_col, st_val, H, out.rp + r, k, out.cap, out.col, out.val, s));
@@ -329,7 +517,13 @@ raptr_status run_build(raptr_ctx* ctx, const int32_t* d_cnl, int64_t n_list, int
   RCU(cudaMemsetAsync(out.rp, 0, sizeof(int64_t), s));
   out.n_list = n_list;
   Builder b{ctx, d_cnl, n_list, nrays, seed, d_rays, (flags & RAPTR_SM_KEEP_ZEROS) != 0, s, out};
-  if (n_list > 0) RCHECK(b.rows(sm_pick_level(ctx->dg, nrays), 0, n_list));
+  if (n_list > 0) {
+    const int level = sm_pick_level(ctx->dg, nrays);
+    if (b.keep_zeros)
+      RCHECK(b.rows(level, 0, n_list));
+    else
+      RCHECK(b.rows_pipelined(level, 0, n_list));
+  }
   RCU(cudaStreamSynchronize(s));
   *nnz_out = b.total;
   if (b.total > out.cap && !out.grow) {
@@ -383,6 +577,7 @@ raptr_status raptr_ctx_destroy(raptr_ctx* ctx) {
   cudaFree(ctx->d_flags);
   cudaFree(ctx->d_f64);
   cudaFree(ctx->d_col_order);
+  cudaFreeHost(ctx->h_pin);
   delete ctx;
   return RAPTR_OK;
 }
@@ -588,6 +783,7 @@ raptr_status transpose_impl(int64_t m, int64_t n, const int64_t* d_row_ptr, cons
     float* st_v = nullptr;
     // plain allocations: the stream-ordered pool grows slowly at these
     // sizes (the staging is tens of GB at full size)
+    const double t0 = trace_on() ? trace_ms() : 0.0;
     cudaError_t e = cudaMalloc(&hist, size_t(nh) * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMalloc(&off, size_t(nh + 1) * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMalloc(&tmp, size_t(scan_temp_elems(std::max(nh, n))) * sizeof(int64_t));
@@ -604,6 +800,7 @@ raptr_status transpose_impl(int64_t m, int64_t n, const int64_t* d_row_ptr, cons
       }
     }
     int32_t h_bad = 0;
+    const double t1 = trace_on() ? trace_ms() : 0.0;
     if (e == cudaSuccess && staged) {
       e = cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
       if (e == cudaSuccess)
@@ -622,6 +819,9 @@ raptr_status transpose_impl(int64_t m, int64_t n, const int64_t* d_row_ptr, cons
     cudaFree(st_key);
     cudaFree(st_k);
     cudaFree(st_v);
+    if (trace_on())
+      trace("transpose radix (%d passes, %s): allocations %.2f ms, sort %.2f ms, total %.2f ms", plan.passes,
+            staged ? "staged" : "staging does not fit", t1 - t0, trace_ms() - t1, trace_ms() - t0);
     if (e != cudaSuccess) return cuda_fail(e, "raptr_csr_transpose");
     if (h_bad) return fail(RAPTR_ERR_INVALID, "column index or row order entry out of range");
     if (staged) return RAPTR_OK;
@@ -716,10 +916,13 @@ raptr_status raptr_matrix_transpose(raptr_matrix* A, void* stream) {
   DeviceScope ds(A->device);
   cudaStream_t s = as_stream(stream);
   bool ordered = false;
+  const double t0 = trace_on() ? trace_ms() : 0.0;
   RCU(matrix_row_order(A, s, &ordered));
+  const double t1 = trace_on() ? trace_ms() : 0.0;
   cudaError_t e = cudaMalloc(&A->cp, size_t(A->n + 1) * sizeof(int64_t));
   if (e == cudaSuccess) e = cudaMalloc(&A->trow, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMalloc(&A->tval, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(float));
+  if (trace_on()) trace("transpose: row order %.2f ms, CSC allocations %.2f ms", t1 - t0, trace_ms() - t1);
   raptr_status st = RAPTR_OK;
   if (e != cudaSuccess)
     st = cuda_fail(e, "cudaMalloc(transpose)");
@@ -984,6 +1187,7 @@ raptr_status mlem_impl(raptr_ctx* ctx, int64_t m, int64_t n, const MlemArrays& A
       e = (e1 != cudaSuccess) ? e1 : e2;
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (trace_on()) trace("mlem: %d iterations captured and instantiated", int(n_iter));
     if (e == cudaSuccess) e = cudaGraphLaunch(exec, cap);
     // the launches were counted when they were captured; the graph runs
     // each of them once
@@ -1405,13 +1609,16 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
   int64_t h2d = M * int64_t(sizeof(float));
   RSTEP(launch_iota(d_list, M, s));
   RSTEP(cudaEventRecord(ev[1], s));
+  trace("reco_host: inputs on the device");
   st = raptr_sm_build_alloc(ctx, d_list, M, nrays, seed, nullptr, 0, &A, s);
+  trace("reco_host: matrix built");
   if (st != RAPTR_OK) {
     std::string msg = g_last_error;
     cleanup();
     return fail(st, msg);
   }
   st = raptr_matrix_transpose(A, s);
+  trace("reco_host: transpose built");
   if (st != RAPTR_OK) {
     std::string msg = g_last_error;
     cleanup();
@@ -1448,7 +1655,9 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
   }
   RSTEP(cudaEventRecord(ev[3], s));
   raptr_mlem_opts o{1, nullptr, nullptr, A->rank};
+  trace("reco_host: sensitivity");
   st = raptr_mlem(ctx, A->m, N, A->rp, A->col, A->val, A->cp, A->trow, A->tval, d_y, d_s, d_x, n_iter, &o, s);
+  trace("reco_host: iterations enqueued");
   if (st != RAPTR_OK) {
     std::string msg = g_last_error;
     cleanup();

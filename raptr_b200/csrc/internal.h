@@ -17,6 +17,13 @@ raptr_status set_error(raptr_status st, const std::string& msg);
 void note_launches(long long k);
 long long launches_so_far();
 
+// Host-side phase trace, enabled by the environment variable RAPTR_TRACE=1:
+// one line per event on stderr, prefixed with the milliseconds since the
+// process's first trace line.  trace_ms() is a host clock in milliseconds.
+bool trace_on();
+void trace(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
+double trace_ms();
+
 // ---- system matrix rows (kernels_sm.cu) ----------------------------------
 
 // Hash/slot capacity levels for the per-channel accumulation table; a row
