@@ -690,6 +690,7 @@ def main():
     # End to end through the public C ABI from host buffers (rank 0, N=1).
     if not args.no_e2e and world == 1:
         times, st = [], None
+        R.reco_host(g, y_full, w["nrays"], SEED, w["niter"], device=dev)  # warm-up, untimed
         for _ in range(max(1, min(args.steps, 2))):
             t0 = time.perf_counter()
             x_h, st = R.reco_host(g, y_full, w["nrays"], SEED, w["niter"], device=dev)

@@ -1567,6 +1567,7 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
                              int32_t n_iter, const float* h_sens, const float* h_x0, float* h_x,
                              raptr_reco_stats* stats) {
   if (!h_y || !h_x || nrays <= 0 || n_iter < 0) return fail(RAPTR_ERR_INVALID, "bad argument");
+  trace("reco_host: start");
   raptr_ctx* ctx = nullptr;
   RCHECK(raptr_ctx_create(geom, device, &ctx));
   DeviceScope ds(device);
@@ -1681,7 +1682,9 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
     stats->d2h_bytes = N * int64_t(sizeof(float));
   }
 #undef RSTEP
+  trace("reco_host: image on the host");
   cleanup();
+  trace("reco_host: device memory released");
   return RAPTR_OK;
 }
 
