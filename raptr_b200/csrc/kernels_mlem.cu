@@ -114,7 +114,25 @@ __device__ __forceinline__ float row_dot_seq(const int32_t* __restrict__ col, co
       acc3 += v[u + 3] * __ldg(x + c[u + 3]);
     }
   }
-  for (; k < e; k += 32) acc0 += __ldcs(val + k) * __ldg(x + __ldcs(col + k));
+  if (k < e) {
+    // the rest of the row (fewer than 32*U entries) as one more step with
+    // predicated loads, so that its loads are in flight together
+    int c[U];
+    float v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const bool in = k + 32 * u < e;
+      c[u] = in ? __ldcs(col + k + 32 * u) : 0;
+      v[u] = in ? __ldcs(val + k + 32 * u) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u += 4) {
+      acc0 += v[u] * __ldg(x + c[u]);
+      acc1 += v[u + 1] * __ldg(x + c[u + 1]);
+      acc2 += v[u + 2] * __ldg(x + c[u + 2]);
+      acc3 += v[u + 3] * __ldg(x + c[u + 3]);
+    }
+  }
   return warp_sum((acc0 + acc1) + (acc2 + acc3));
 }
 

@@ -137,8 +137,24 @@ __device__ __forceinline__ float row_dot_half(const int32_t* __restrict__ col, c
       acc3 += h2f(v[u + 3]) * __ldg(x + c[u + 3]);
     }
   }
-  for (; k < e; k += 32)
-    acc0 += h2f(__ldcs(reinterpret_cast<const unsigned short*>(hv) + k)) * __ldg(x + __ldcs(col + k));
+  if (k < e) {
+    // the rest of the row as one more step with predicated loads
+    int c[U];
+    uint16_t v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const bool in = k + 32 * u < e;
+      c[u] = in ? __ldcs(col + k + 32 * u) : 0;
+      v[u] = in ? __ldcs(reinterpret_cast<const unsigned short*>(hv) + k + 32 * u) : uint16_t(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u += 4) {
+      acc0 += h2f(v[u]) * __ldg(x + c[u]);
+      acc1 += h2f(v[u + 1]) * __ldg(x + c[u + 1]);
+      acc2 += h2f(v[u + 2]) * __ldg(x + c[u + 2]);
+      acc3 += h2f(v[u + 3]) * __ldg(x + c[u + 3]);
+    }
+  }
   return warp_sum_f((acc0 + acc1) + (acc2 + acc3));
 }
 
