@@ -11,12 +11,15 @@
 //      reference's intersectionLength (src/getSystemMatrixDeviceOnly.cu:129-174):
 //      per-axis plane parameters (face - start)/(end - start), masked max of
 //      the entry parameters, masked min of the exit parameters, and
-//      (exit - entry) * |end - start|.  Lengths are summed into a per-row
-//      open-addressing hash table in shared memory keyed by voxel id;
-//   3. the table is compacted keeping voxels that pass the exact cylinder
+//      (exit - entry) * |end - start|.  Lengths are summed in shared memory:
+//      into dense per-slab windows of the voxels the row's rays can reach
+//      when the two crystals lie on opposite sides of the grid along x or z,
+//      else into an open-addressing hash table keyed by voxel id;
+//   3. the sums are compacted keeping voxels that pass the exact cylinder
 //      test (the reference only evaluates candidates,
-//      src/getSystemMatrixDeviceOnly.cu:433-470), bitonic-sorted by voxel id,
-//      divided by the ray count and written to the row's staging slot.
+//      src/getSystemMatrixDeviceOnly.cu:433-470), put in voxel-id order
+//      (x-slab windows already are; the others are bitonic-sorted), divided
+//      by the ray count and written to the row's staging slot.
 // The rows are therefore emitted already in (row, column) order: no global
 // COO sort (src/cooSort.hpp:75-99) and no coo->csr pass are needed; a scan
 // of the row lengths and a gather place them into CSR.
