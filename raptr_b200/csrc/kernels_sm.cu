@@ -456,6 +456,16 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total, int* warp
 
 constexpr int kMaxSlabs = 256;
 
+// Dense slots of a row (floats) and the row kernel's dynamic shared memory:
+// the hash table's H keys and H sums, or the dense windows, whichever is
+// larger.  3H dense slots keep every row of the centred-cube workloads
+// dense; at H = 4096 the 48 KB still leave four CTAs per SM, which the
+// registers limit it to anyway.
+__host__ __device__ constexpr int dense_slots(int H) { return H <= 4096 ? 3 * H : 2 * H; }
+__host__ __device__ constexpr size_t row_smem_bytes(int H) {
+  return size_t(H) * 8 > size_t(dense_slots(H)) * 4 ? size_t(H) * 8 : size_t(dense_slots(H)) * 4;
+}
+
 // Row-level decision for the slab windows: both crystals' boxes (corner
 // AABBs) lie on opposite sides of the grid in x, so every ray of the row
 // crosses the whole grid in the same x direction (xdir) and lies in the
@@ -514,8 +524,8 @@ __device__ inline void slab_window(const DGeom& g, int a, const float plo[3], co
 // their lengths summed per voxel in shared memory, then the voxels that pass
 // the cylinder test are written in column order to the row's staging slot.
 // The sums go to dense slab windows when the row allows it (generated rays,
-// crystals on opposite sides of the grid along x or z, windows within 2H
-// slots), else to an open-addressing hash table of H keys; a dense row that
+// crystals on opposite sides of the grid along x or z, windows within
+// dense_slots(H) slots), else to an open-addressing hash table of H keys; a dense row that
 // finds a voxel outside its windows is redone with the table.
 template <int H, int T, bool OISO>
 __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __restrict__ sincos,
@@ -526,7 +536,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
   extern __shared__ __align__(16) unsigned char smem[];
   int* keys = reinterpret_cast<int*>(smem);
   float* vals = reinterpret_cast<float*>(smem + H * sizeof(int));
-  float* acc = reinterpret_cast<float*>(smem);  // dense mode: 2H slots over both arrays
+  float* acc = reinterpret_cast<float*>(smem);  // dense mode: dense_slots(H) slots over the same memory
   __shared__ Channel ch;
   __shared__ int overflow, bad_walk, dense_fail, win_u, win_v, sax, sdir;
   __shared__ float box_lo[2][3], box_hi[2][3];
@@ -556,9 +566,12 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     int axis = -1, dir = 0;
     if (!rays) {
       crystal_boxes(ch, box_lo, box_hi);
-      // the slab axis: x if the crystals lie on opposite x sides of the
-      // grid, else z if they do along z
-      for (int a = 0; a <= 2 && axis < 0; a += 2) {
+      // the slab axis: of x and z, the one along which the crystals lie
+      // on opposite sides of the grid, the channel's dominant direction
+      // first (its windows are the narrowest)
+      const int first = fabsf(ch.ab[0]) >= fabsf(ch.ab[2]) ? 0 : 2;
+      for (int k = 0; k < 2 && axis < 0; k++) {
+        const int a = k == 0 ? first : 2 - first;
         if (g.n[a] > kMaxSlabs) continue;
         const float c0 = g.o[a], c1 = g.o[a] + float(g.n[a]) * g.d[a];
         const float m = 1e-6f * (1.0f + fabsf(c0) + fabsf(c1));
@@ -591,7 +604,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
   }
   const int wu = win_u, wv = win_v;
   const int wuv = wu * wv;
-  bool use_dense = A >= 0 && (long long)na * wuv <= 2LL * H;
+  bool use_dense = A >= 0 && (long long)na * wuv <= (long long)dense_slots(H);
   const int nslots = use_dense ? na * wuv : 0;
 
   const float fr = float(nrays);
@@ -826,7 +839,7 @@ template <int H, int T>
 cudaError_t launch_level(const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0, int64_t nrows,
                          int nrays, uint32_t seed, const float* d_rays, int32_t* st_col, float* st_val,
                          int32_t* row_nnz, int32_t* d_flags, cudaStream_t s) {
-  const size_t smem = size_t(H) * (sizeof(int) + sizeof(float));
+  const size_t smem = row_smem_bytes(H);
   // A grid with the same origin on every axis (the usual centred cube) lets
   // the walk's step skip selecting the origin.
   const bool oiso = g.o[0] == g.o[1] && g.o[1] == g.o[2];
