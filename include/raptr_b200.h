@@ -79,6 +79,18 @@ const char* raptr_last_error(void);
  * replayed from a CUDA graph included). */
 int64_t raptr_kernel_launches(void);
 
+/* No counterpart in the reference (it frees its buffers with cudaFree).
+ * Device blocks of 64 MB and more that the library frees (matrices, their
+ * transposes, transpose staging, build scratch) are kept for reuse by its
+ * next allocations of a similar size, up to half of each device's memory,
+ * because freeing and reallocating tens of GB per reconstruction job costs
+ * host time while the device idles.  Freeing still waits for the device's
+ * work, as cudaFree does.  raptr_trim_memory returns the kept blocks of
+ * `device` (-1: every device) to the driver, e.g. before the caller
+ * allocates much device memory by other means; the library also does so by
+ * itself when one of its allocations fails. */
+raptr_status raptr_trim_memory(int device);
+
 raptr_status raptr_ctx_create(const raptr_geom* geom, int device, raptr_ctx** out);
 raptr_status raptr_ctx_destroy(raptr_ctx* ctx);
 int64_t raptr_ctx_num_channels(const raptr_ctx* ctx);

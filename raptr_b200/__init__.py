@@ -106,6 +106,7 @@ _SIGNATURES = {
     "raptr_abi_version": (C.c_int, []),
     "raptr_last_error": (C.c_char_p, []),
     "raptr_kernel_launches": (I64, []),
+    "raptr_trim_memory": (I32, [I32]),
     "raptr_ctx_create": (C.c_int, [C.POINTER(raptr_geom), C.c_int, C.POINTER(VP)]),
     "raptr_ctx_destroy": (C.c_int, [VP]),
     "raptr_ctx_num_channels": (I64, [VP]),
@@ -649,6 +650,12 @@ def kernel_launches() -> int:
     return lib().raptr_kernel_launches()
 
 
+def trim_memory(device: int = -1) -> None:
+    """Returns the device blocks the library keeps for reuse (freed
+    matrices, transpose staging) to the driver; -1: every device."""
+    _check(lib().raptr_trim_memory(device))
+
+
 def reco_host(geom: Geometry, y: np.ndarray, nrays: int, seed: int, niter: int, sens: Optional[np.ndarray] = None,
               x0: Optional[np.ndarray] = None, device: int = 0):
     """The reco flow from host arrays: returns (x, stats dict)."""
@@ -669,5 +676,5 @@ def reco_host(geom: Geometry, y: np.ndarray, nrays: int, seed: int, niter: int, 
 __all__ = [
     "Geometry", "SMALL", "FULL", "FINE", "WORKLOADS", "epet_geometry", "phantom", "poisson_measurement", "Context",
     "Matrix", "spmv", "sensitivity", "mlem_project", "mlem_forward", "mlem_back", "csr_transpose", "mlem_update", "divides", "divides_multiplies", "scales",
-    "vsum", "coo2csr", "csr2ecsr", "reco_host", "lib", "RaptrError", "OP_N", "OP_T",
+    "vsum", "coo2csr", "csr2ecsr", "reco_host", "lib", "RaptrError", "OP_N", "OP_T", "trim_memory",
 ]

@@ -31,6 +31,7 @@ UNITS = {
     "kernels_batch.cu": [],
     "server.cu": [],
     "h5lite.cpp": [],
+    "devmem.cu": [],
     "mlem_noalloc.cu": [],
 }
 

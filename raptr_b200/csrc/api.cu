@@ -175,10 +175,10 @@ struct raptr_ctx {
           for (int x = 0; x < nx; x++)
             for (int y = ty; y < std::min(ny, ty + tb); y++)
               for (int z = tz; z < std::min(nz, tz + tb); z++) h.push_back(int32_t((int64_t(x) * ny + y) * nz + z));
-      cudaError_t e = cudaMalloc(&d_col_order, h.size() * sizeof(int32_t));
+      cudaError_t e = dev_malloc(&d_col_order, h.size() * sizeof(int32_t));
       if (e == cudaSuccess) e = cudaMemcpy(d_col_order, h.data(), h.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
       if (e != cudaSuccess) {
-        cudaFree(d_col_order);
+        dev_free(d_col_order);
         d_col_order = nullptr;
         return e;
       }
@@ -189,11 +189,11 @@ struct raptr_ctx {
 
   raptr_status ensure_scratch(size_t bytes) {
     if (bytes <= scratch_bytes) return RAPTR_OK;
-    if (d_scratch) cudaFree(d_scratch);
+    if (d_scratch) dev_free(d_scratch);
     d_scratch = nullptr;
     scratch_bytes = 0;
     size_t want = std::max(bytes, size_t(64) << 20);
-    RCU(cudaMalloc(&d_scratch, want));
+    RCU(dev_malloc(&d_scratch, want));
     scratch_bytes = want;
     return RAPTR_OK;
   }
@@ -269,10 +269,10 @@ raptr_status ensure_capacity(BuildOut& o, int64_t need, int64_t rows_done, cudaS
   const double t0 = trace_on() ? trace_ms() : 0.0;
   int32_t* ncol = nullptr;
   float* nval = nullptr;
-  RCU(cudaMalloc(&ncol, size_t(ncap) * sizeof(int32_t)));
-  cudaError_t e = cudaMalloc(&nval, size_t(ncap) * sizeof(float));
+  RCU(dev_malloc(&ncol, size_t(ncap) * sizeof(int32_t)));
+  cudaError_t e = dev_malloc(&nval, size_t(ncap) * sizeof(float));
   if (e != cudaSuccess) {
-    cudaFree(ncol);
+    dev_free(ncol);
     return cuda_fail(e, "cudaMalloc(matrix values)");
   }
   int64_t keep = std::min(o.cap, need);
@@ -281,8 +281,8 @@ raptr_status ensure_capacity(BuildOut& o, int64_t need, int64_t rows_done, cudaS
     RCU(cudaMemcpyAsync(nval, o.val, size_t(keep) * sizeof(float), cudaMemcpyDeviceToDevice, s));
   }
   RCU(cudaStreamSynchronize(s));
-  if (o.col) cudaFree(o.col);
-  if (o.val) cudaFree(o.val);
+  if (o.col) dev_free(o.col);
+  if (o.val) dev_free(o.val);
   o.col = ncol;
   o.val = nval;
   o.cap = ncap;
@@ -539,6 +539,11 @@ extern "C" {
 
 int raptr_abi_version(void) { return RAPTR_ABI_VERSION; }
 
+raptr_status raptr_trim_memory(int device) {
+  dev_release(device < 0 ? -1 : device);
+  return RAPTR_OK;
+}
+
 const char* raptr_last_error(void) { return g_last_error.c_str(); }
 
 int64_t raptr_kernel_launches(void) { return launches_so_far(); }
@@ -555,11 +560,11 @@ raptr_status raptr_ctx_create(const raptr_geom* geom, int device, raptr_ctx** ou
   c->device = device;
   std::vector<float2> tab;
   sincos_table(*geom, tab);
-  cudaError_t e = cudaMalloc(&c->d_sincos, tab.size() * sizeof(float2));
+  cudaError_t e = dev_malloc(&c->d_sincos, tab.size() * sizeof(float2));
   if (e == cudaSuccess) e = cudaMemcpy(c->d_sincos, tab.data(), tab.size() * sizeof(float2), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMalloc(&c->d_i64, 64 * sizeof(int64_t));
-  if (e == cudaSuccess) e = cudaMalloc(&c->d_flags, 16 * sizeof(int32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&c->d_f64, 64 * sizeof(double));
+  if (e == cudaSuccess) e = dev_malloc(&c->d_i64, 64 * sizeof(int64_t));
+  if (e == cudaSuccess) e = dev_malloc(&c->d_flags, 16 * sizeof(int32_t));
+  if (e == cudaSuccess) e = dev_malloc(&c->d_f64, 64 * sizeof(double));
   if (e != cudaSuccess) {
     raptr_ctx_destroy(c);
     return cuda_fail(e, "context allocation");
@@ -571,12 +576,12 @@ raptr_status raptr_ctx_create(const raptr_geom* geom, int device, raptr_ctx** ou
 raptr_status raptr_ctx_destroy(raptr_ctx* ctx) {
   if (!ctx) return RAPTR_OK;
   DeviceScope ds(ctx->device);
-  cudaFree(ctx->d_sincos);
-  cudaFree(ctx->d_scratch);
-  cudaFree(ctx->d_i64);
-  cudaFree(ctx->d_flags);
-  cudaFree(ctx->d_f64);
-  cudaFree(ctx->d_col_order);
+  dev_free(ctx->d_sincos);
+  dev_free(ctx->d_scratch);
+  dev_free(ctx->d_i64);
+  dev_free(ctx->d_flags);
+  dev_free(ctx->d_f64);
+  dev_free(ctx->d_col_order);
   cudaFreeHost(ctx->h_pin);
   delete ctx;
   return RAPTR_OK;
@@ -700,7 +705,7 @@ raptr_status raptr_sm_build_alloc(raptr_ctx* ctx, const int32_t* d_cnl_ids, int6
   A->device = ctx->device;
   A->m = n_list;
   A->n = raptr_ctx_num_voxels(ctx);
-  cudaError_t e = cudaMalloc(&A->rp, size_t(n_list + 1) * sizeof(int64_t));
+  cudaError_t e = dev_malloc(&A->rp, size_t(n_list + 1) * sizeof(int64_t));
   if (e != cudaSuccess) {
     delete A;
     return cuda_fail(e, "cudaMalloc(row pointers)");
@@ -717,7 +722,7 @@ raptr_status raptr_sm_build_alloc(raptr_ctx* ctx, const int32_t* d_cnl_ids, int6
   A->nnz = nnz;
   A->geom = ctx->dg;
   if (n_list > 0) {
-    cudaError_t ec = cudaMalloc(&A->cnl, size_t(n_list) * sizeof(int32_t));
+    cudaError_t ec = dev_malloc(&A->cnl, size_t(n_list) * sizeof(int32_t));
     if (ec == cudaSuccess)
       ec = cudaMemcpyAsync(A->cnl, d_cnl_ids, size_t(n_list) * sizeof(int32_t), cudaMemcpyDeviceToDevice,
                            as_stream(stream));
@@ -745,19 +750,21 @@ raptr_status raptr_matrix_info(const raptr_matrix* A, int64_t* m, int64_t* n, in
 raptr_status raptr_matrix_destroy(raptr_matrix* A) {
   if (!A) return RAPTR_OK;
   DeviceScope ds(A->device);
-  cudaFree(A->rp);
-  cudaFree(A->col);
-  cudaFree(A->val);
-  cudaFree(A->cp);
-  cudaFree(A->trow);
-  cudaFree(A->tval);
-  cudaFree(A->cnl);
-  cudaFree(A->rank);
-  cudaFree(A->order);
-  cudaFree(A->rscale);
-  cudaFree(A->pscale);
-  cudaFree(A->hval);
-  cudaFree(A->htval);
+  const double t0 = trace_on() ? trace_ms() : 0.0;
+  dev_free(A->rp);
+  dev_free(A->col);
+  dev_free(A->val);
+  dev_free(A->cp);
+  dev_free(A->trow);
+  dev_free(A->tval);
+  dev_free(A->cnl);
+  dev_free(A->rank);
+  dev_free(A->order);
+  dev_free(A->rscale);
+  dev_free(A->pscale);
+  dev_free(A->hval);
+  dev_free(A->htval);
+  if (trace_on()) trace("matrix released: %.2f ms", trace_ms() - t0);
   delete A;
   return RAPTR_OK;
 }
@@ -784,17 +791,17 @@ raptr_status transpose_impl(int64_t m, int64_t n, const int64_t* d_row_ptr, cons
     // plain allocations: the stream-ordered pool grows slowly at these
     // sizes (the staging is tens of GB at full size)
     const double t0 = trace_on() ? trace_ms() : 0.0;
-    cudaError_t e = cudaMalloc(&hist, size_t(nh) * sizeof(int64_t));
-    if (e == cudaSuccess) e = cudaMalloc(&off, size_t(nh + 1) * sizeof(int64_t));
-    if (e == cudaSuccess) e = cudaMalloc(&tmp, size_t(scan_temp_elems(std::max(nh, n))) * sizeof(int64_t));
-    if (e == cudaSuccess) e = cudaMalloc(&cc, size_t(n) * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&cc64, size_t(n) * sizeof(int64_t));
-    if (e == cudaSuccess) e = cudaMalloc(&bad, sizeof(int32_t));
+    cudaError_t e = dev_malloc(&hist, size_t(nh) * sizeof(int64_t));
+    if (e == cudaSuccess) e = dev_malloc(&off, size_t(nh + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = dev_malloc(&tmp, size_t(scan_temp_elems(std::max(nh, n))) * sizeof(int64_t));
+    if (e == cudaSuccess) e = dev_malloc(&cc, size_t(n) * sizeof(int32_t));
+    if (e == cudaSuccess) e = dev_malloc(&cc64, size_t(n) * sizeof(int64_t));
+    if (e == cudaSuccess) e = dev_malloc(&bad, sizeof(int32_t));
     bool staged = true;
     if (e == cudaSuccess && plan.passes > 1) {
-      if (cudaMalloc(&st_key, size_t(nnz) * sizeof(int32_t)) != cudaSuccess ||
-          cudaMalloc(&st_k, size_t(nnz) * sizeof(int32_t)) != cudaSuccess ||
-          cudaMalloc(&st_v, size_t(nnz) * sizeof(float)) != cudaSuccess) {
+      if (dev_malloc(&st_key, size_t(nnz) * sizeof(int32_t)) != cudaSuccess ||
+          dev_malloc(&st_k, size_t(nnz) * sizeof(int32_t)) != cudaSuccess ||
+          dev_malloc(&st_v, size_t(nnz) * sizeof(float)) != cudaSuccess) {
         (void)cudaGetLastError();  // does not fit: the blocked transpose needs less
         staged = false;
       }
@@ -810,18 +817,20 @@ raptr_status transpose_impl(int64_t m, int64_t n, const int64_t* d_row_ptr, cons
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     }
     cudaStreamSynchronize(s);
-    cudaFree(hist);
-    cudaFree(off);
-    cudaFree(tmp);
-    cudaFree(cc);
-    cudaFree(cc64);
-    cudaFree(bad);
-    cudaFree(st_key);
-    cudaFree(st_k);
-    cudaFree(st_v);
+    const double t2 = trace_on() ? trace_ms() : 0.0;
+    dev_free(hist);
+    dev_free(off);
+    dev_free(tmp);
+    dev_free(cc);
+    dev_free(cc64);
+    dev_free(bad);
+    dev_free(st_key);
+    dev_free(st_k);
+    dev_free(st_v);
     if (trace_on())
-      trace("transpose radix (%d passes, %s): allocations %.2f ms, sort %.2f ms, total %.2f ms", plan.passes,
-            staged ? "staged" : "staging does not fit", t1 - t0, trace_ms() - t1, trace_ms() - t0);
+      trace("transpose radix (%d passes, %s): allocations %.2f ms, sort %.2f ms, release %.2f ms, total %.2f ms",
+            plan.passes, staged ? "staged" : "staging does not fit", t1 - t0, t2 - t1, trace_ms() - t2,
+            trace_ms() - t0);
     if (e != cudaSuccess) return cuda_fail(e, "raptr_csr_transpose");
     if (h_bad) return fail(RAPTR_ERR_INVALID, "column index or row order entry out of range");
     if (staged) return RAPTR_OK;
@@ -878,11 +887,13 @@ cudaError_t matrix_row_order(raptr_matrix* A, cudaStream_t s, bool* have) {
   unsigned long long* mark = nullptr;
   int64_t *prefix = nullptr, *tmp = nullptr;
   int32_t* bad = nullptr;
+  const double t0 = trace_on() ? trace_ms() : 0.0;
   // plain allocations: the stream-ordered pool grows slowly at this size
-  cudaError_t e = cudaMalloc(&mark, size_t(K) * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMalloc(&prefix, size_t(K + 1) * sizeof(int64_t));
-  if (e == cudaSuccess) e = cudaMalloc(&tmp, size_t(scan_temp_elems(K)) * sizeof(int64_t));
-  if (e == cudaSuccess) e = cudaMalloc(&bad, sizeof(int32_t));
+  cudaError_t e = dev_malloc(&mark, size_t(K) * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = dev_malloc(&prefix, size_t(K + 1) * sizeof(int64_t));
+  if (e == cudaSuccess) e = dev_malloc(&tmp, size_t(scan_temp_elems(K)) * sizeof(int64_t));
+  if (e == cudaSuccess) e = dev_malloc(&bad, sizeof(int32_t));
+  const double t1 = trace_on() ? trace_ms() : 0.0;
   if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
   if (e == cudaSuccess) e = launch_channel_order_mark(A->geom, A->m, A->cnl, mark, bad, s);
   if (e == cudaSuccess) e = launch_scan_i64(reinterpret_cast<const int64_t*>(mark), K, prefix, tmp, s);
@@ -890,21 +901,25 @@ cudaError_t matrix_row_order(raptr_matrix* A, cudaStream_t s, bool* have) {
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e == cudaSuccess && !h_bad) {
-    e = cudaMalloc(&A->rank, size_t(A->m) * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&A->order, size_t(A->m) * sizeof(int32_t));
+    e = dev_malloc(&A->rank, size_t(A->m) * sizeof(int32_t));
+    if (e == cudaSuccess) e = dev_malloc(&A->order, size_t(A->m) * sizeof(int32_t));
     if (e == cudaSuccess) e = launch_channel_order_rank(A->geom, A->m, A->cnl, prefix, A->rank, A->order, s);
     if (e == cudaSuccess) {
       *have = true;
     } else {
-      cudaFree(A->rank);
-      cudaFree(A->order);
+      dev_free(A->rank);
+      dev_free(A->order);
       A->rank = A->order = nullptr;
     }
   }
-  cudaFree(mark);
-  cudaFree(prefix);
-  cudaFree(tmp);
-  cudaFree(bad);
+  const double t2 = trace_on() ? trace_ms() : 0.0;
+  dev_free(mark);
+  dev_free(prefix);
+  dev_free(tmp);
+  dev_free(bad);
+  if (trace_on())
+    trace("row order: allocations %.2f ms, keys and ranks %.2f ms, release %.2f ms", t1 - t0, t2 - t1,
+          trace_ms() - t2);
   return e;
 }
 
@@ -919,9 +934,9 @@ raptr_status raptr_matrix_transpose(raptr_matrix* A, void* stream) {
   const double t0 = trace_on() ? trace_ms() : 0.0;
   RCU(matrix_row_order(A, s, &ordered));
   const double t1 = trace_on() ? trace_ms() : 0.0;
-  cudaError_t e = cudaMalloc(&A->cp, size_t(A->n + 1) * sizeof(int64_t));
-  if (e == cudaSuccess) e = cudaMalloc(&A->trow, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(int32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&A->tval, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(float));
+  cudaError_t e = dev_malloc(&A->cp, size_t(A->n + 1) * sizeof(int64_t));
+  if (e == cudaSuccess) e = dev_malloc(&A->trow, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(int32_t));
+  if (e == cudaSuccess) e = dev_malloc(&A->tval, size_t(std::max<int64_t>(A->nnz, 1)) * sizeof(float));
   if (trace_on()) trace("transpose: row order %.2f ms, CSC allocations %.2f ms", t1 - t0, trace_ms() - t1);
   raptr_status st = RAPTR_OK;
   if (e != cudaSuccess)
@@ -929,11 +944,11 @@ raptr_status raptr_matrix_transpose(raptr_matrix* A, void* stream) {
   else
     st = transpose_impl(A->m, A->n, A->rp, A->col, A->val, ordered ? A->order : nullptr, A->cp, A->trow, A->tval, s);
   if (st != RAPTR_OK) {
-    cudaFree(A->cp);
-    cudaFree(A->trow);
-    cudaFree(A->tval);
-    cudaFree(A->rank);
-    cudaFree(A->order);
+    dev_free(A->cp);
+    dev_free(A->trow);
+    dev_free(A->tval);
+    dev_free(A->rank);
+    dev_free(A->order);
     A->cp = nullptr;
     A->trow = nullptr;
     A->tval = nullptr;
@@ -1306,19 +1321,19 @@ raptr_status raptr_matrix_half(raptr_matrix* A, void* stream) {
   DeviceScope ds(A->device);
   cudaStream_t s = as_stream(stream);
   const size_t mm = size_t(std::max<int64_t>(A->m, 1)), nz = size_t(std::max<int64_t>(A->nnz, 1));
-  cudaError_t e = cudaMalloc(&A->rscale, mm * sizeof(float));
-  if (e == cudaSuccess) e = cudaMalloc(&A->pscale, mm * sizeof(float));
-  if (e == cudaSuccess) e = cudaMalloc(&A->hval, nz * sizeof(uint16_t));
-  if (e == cudaSuccess) e = cudaMalloc(&A->htval, nz * sizeof(uint16_t));
+  cudaError_t e = dev_malloc(&A->rscale, mm * sizeof(float));
+  if (e == cudaSuccess) e = dev_malloc(&A->pscale, mm * sizeof(float));
+  if (e == cudaSuccess) e = dev_malloc(&A->hval, nz * sizeof(uint16_t));
+  if (e == cudaSuccess) e = dev_malloc(&A->htval, nz * sizeof(uint16_t));
   if (e == cudaSuccess)
     e = launch_half_convert(A->m, A->nnz, A->rp, A->val, A->trow, A->tval, A->order, A->rscale, A->hval, A->htval,
                             A->pscale, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
-    cudaFree(A->rscale);
-    cudaFree(A->pscale);
-    cudaFree(A->hval);
-    cudaFree(A->htval);
+    dev_free(A->rscale);
+    dev_free(A->pscale);
+    dev_free(A->hval);
+    dev_free(A->htval);
     A->rscale = A->pscale = nullptr;
     A->hval = A->htval = nullptr;
     return cuda_fail(e, "raptr_matrix_half");
@@ -1340,8 +1355,8 @@ raptr_status raptr_matrix_drop_f32(raptr_matrix* A) {
   if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
   if (!A->hval) return fail(RAPTR_ERR_INVALID, "the FP32 values are the only ones: call raptr_matrix_half first");
   DeviceScope ds(A->device);
-  cudaFree(A->val);
-  cudaFree(A->tval);
+  dev_free(A->val);
+  dev_free(A->tval);
   A->val = nullptr;
   A->tval = nullptr;
   return RAPTR_OK;
@@ -1583,11 +1598,11 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
   raptr_status st = RAPTR_OK;
   auto cleanup = [&]() {
     raptr_matrix_destroy(A);
-    cudaFree(d_y);
-    cudaFree(d_x);
-    cudaFree(d_s);
-    cudaFree(d_list);
-    cudaFree(d_s64);
+    dev_free(d_y);
+    dev_free(d_x);
+    dev_free(d_s);
+    dev_free(d_list);
+    dev_free(d_s64);
     for (auto& e : ev) cudaEventDestroy(e);
     cudaStreamDestroy(s);
     raptr_ctx_destroy(ctx);
@@ -1602,10 +1617,10 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
     }                                                       \
   } while (0)
   RSTEP(cudaEventRecord(ev[0], s));
-  RSTEP(cudaMalloc(&d_y, size_t(M) * sizeof(float)));
-  RSTEP(cudaMalloc(&d_x, size_t(N) * sizeof(float)));
-  RSTEP(cudaMalloc(&d_s, size_t(N) * sizeof(float)));
-  RSTEP(cudaMalloc(&d_list, size_t(M) * sizeof(int32_t)));
+  RSTEP(dev_malloc(&d_y, size_t(M) * sizeof(float)));
+  RSTEP(dev_malloc(&d_x, size_t(N) * sizeof(float)));
+  RSTEP(dev_malloc(&d_s, size_t(N) * sizeof(float)));
+  RSTEP(dev_malloc(&d_list, size_t(M) * sizeof(int32_t)));
   RSTEP(cudaMemcpyAsync(d_y, h_y, size_t(M) * sizeof(float), cudaMemcpyHostToDevice, s));
   int64_t h2d = M * int64_t(sizeof(float));
   RSTEP(launch_iota(d_list, M, s));
@@ -1627,7 +1642,7 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
   }
   RSTEP(cudaEventRecord(ev[2], s));
   if (!h_sens) {
-    RSTEP(cudaMalloc(&d_s64, size_t(N) * sizeof(double)));
+    RSTEP(dev_malloc(&d_s64, size_t(N) * sizeof(double)));
     st = raptr_sensitivity(A->m, N, A->rp, A->col, A->val, d_s64, d_s, s);
   } else {
     RSTEP(cudaMemcpyAsync(d_s, h_sens, size_t(N) * sizeof(float), cudaMemcpyHostToDevice, s));

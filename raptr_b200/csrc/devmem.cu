@@ -1,0 +1,125 @@
+// Device memory for the library's large buffers (system matrices, their
+// transposes, transpose staging, build scratch), kept for reuse when freed.
+//
+// A reconstruction job allocates and frees tens of GB per build and
+// transpose; cudaFree of such blocks costs 30-600 ms of host time during
+// which the device idles, and a job that follows reallocates the same
+// sizes.  Blocks of at least kMinCached bytes are therefore not returned
+// to the driver when the library frees them but parked per device, and a
+// later request of a similar size (up to 25 % smaller) takes the smallest
+// fitting parked block.  Parked bytes per device are capped at half the
+// device's memory; when an allocation fails, the device's parked blocks
+// are released and the allocation is retried once.  raptr_trim_memory()
+// releases them on request (before a caller allocates much memory by other
+// means, say).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <unordered_map>
+
+#include "internal.h"
+
+namespace raptr {
+
+namespace {
+
+constexpr size_t kMinCached = size_t(64) << 20;
+
+struct Block {
+  size_t bytes;
+  int device;
+};
+
+std::mutex g_mu;
+std::unordered_map<void*, Block> g_live;                 // large blocks handed out
+std::map<int, std::multimap<size_t, void*>> g_parked;    // device -> size -> block
+std::map<int, size_t> g_parked_bytes;
+std::map<int, size_t> g_total;                           // device -> memory size
+
+// Releases the parked blocks of `device` (all devices for -1).  Holds g_mu.
+void release_locked(int device) {
+  int cur = -1;
+  cudaGetDevice(&cur);
+  for (auto it = g_parked.begin(); it != g_parked.end(); ++it) {
+    if (device >= 0 && it->first != device) continue;
+    cudaSetDevice(it->first);
+    for (auto& kv : it->second) cudaFree(kv.second);
+    it->second.clear();
+    g_parked_bytes[it->first] = 0;
+  }
+  if (cur >= 0) cudaSetDevice(cur);
+}
+
+}  // namespace
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes < kMinCached) return cudaMalloc(p, bytes);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_mu);
+  auto& parked = g_parked[dev];
+  auto it = parked.lower_bound(bytes);
+  if (it != parked.end() && it->first <= bytes + bytes / 4) {
+    *p = it->second;
+    g_live[*p] = Block{it->first, dev};
+    g_parked_bytes[dev] -= it->first;
+    parked.erase(it);
+    return cudaSuccess;
+  }
+  e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation && !parked.empty()) {
+    (void)cudaGetLastError();
+    release_locked(dev);
+    e = cudaMalloc(p, bytes);
+  }
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return e;
+  }
+  g_live[*p] = Block{bytes, dev};
+  return cudaSuccess;
+}
+
+void dev_free(void* p) {
+  if (!p) return;
+  std::unique_lock<std::mutex> lock(g_mu);
+  auto it = g_live.find(p);
+  if (it == g_live.end()) {
+    lock.unlock();
+    cudaFree(p);
+    return;
+  }
+  const Block b = it->second;
+  g_live.erase(it);
+  size_t total = 0, freeb = 0;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != b.device) cudaSetDevice(b.device);
+  // like cudaFree, wait for the device's work (which may still use the
+  // block) before the block can be handed out again
+  bool info = cudaDeviceSynchronize() == cudaSuccess;
+  if (info && !g_total.count(b.device)) {
+    info = cudaMemGetInfo(&freeb, &total) == cudaSuccess;
+    if (info) g_total[b.device] = total;
+  }
+  if (info) total = g_total[b.device];
+  if (info && g_parked_bytes[b.device] + b.bytes <= total / 2) {
+    g_parked[b.device].emplace(b.bytes, p);
+    g_parked_bytes[b.device] += b.bytes;
+  } else {
+    (void)cudaGetLastError();
+    cudaFree(p);
+  }
+  if (cur >= 0 && cur != b.device) cudaSetDevice(cur);
+}
+
+void dev_release(int device) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  release_locked(device);
+}
+
+}  // namespace raptr

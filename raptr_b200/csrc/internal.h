@@ -17,6 +17,21 @@ raptr_status set_error(raptr_status st, const std::string& msg);
 void note_launches(long long k);
 long long launches_so_far();
 
+// Device allocations of the library (devmem.cpp): blocks of 64 MB and more
+// are parked for reuse when freed instead of going back to the driver;
+// dev_free waits for the device like cudaFree.  dev_release returns the
+// parked blocks of a device (-1: all) to the driver.
+cudaError_t dev_alloc(void** p, size_t bytes);
+void dev_free(void* p);
+void dev_release(int device);
+template <class T>
+cudaError_t dev_malloc(T** p, size_t bytes) {
+  void* q = nullptr;
+  cudaError_t e = dev_alloc(&q, bytes);
+  *p = static_cast<T*>(q);
+  return e;
+}
+
 // Host-side phase trace, enabled by the environment variable RAPTR_TRACE=1:
 // one line per event on stderr, prefixed with the milliseconds since the
 // process's first trace line.  trace_ms() is a host clock in milliseconds.

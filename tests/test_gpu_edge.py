@@ -117,3 +117,33 @@ def test_zero_iterations_leave_the_image(rlib, torch):
     x0 = x.clone()
     ctx.mlem(A, y, s, x, 0)
     assert torch.equal(x, x0)
+
+
+def test_freed_blocks_are_reused_and_trimmed(rlib, torch):
+    # Large blocks the library frees are kept for its next allocations;
+    # a rebuild into them gives the same matrix, and trim_memory hands them
+    # back to the driver.
+    import gc
+
+    g = cfg.FULL
+    ctx = rlib.Context(g, 0)
+    lst = np.arange(60000, dtype=np.int32)
+    A = ctx.build(lst, 200, 1251)
+    A.transpose()
+    rp0, col0, val0 = A.to_numpy()
+    assert col0.nbytes >= (64 << 20)
+    del A
+    gc.collect()
+    torch.cuda.synchronize()
+    B = ctx.build(lst, 200, 1251)
+    B.transpose()
+    rp1, col1, val1 = B.to_numpy()
+    assert np.array_equal(rp0, rp1) and np.array_equal(col0, col1)
+    assert np.allclose(val0, val1, rtol=1e-6, atol=0)
+    del B
+    gc.collect()
+    torch.cuda.synchronize()
+    free_kept = torch.cuda.mem_get_info()[0]
+    rlib.trim_memory()
+    free_trimmed = torch.cuda.mem_get_info()[0]
+    assert free_trimmed - free_kept >= 2 * col0.nbytes

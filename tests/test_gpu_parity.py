@@ -492,11 +492,13 @@ def test_full_size_matrix_properties(rlib, oracle, torch, ctx_full):
 
 def test_matrix_memory_is_released(rlib, torch, ctx_small):
     """Device memory of a matrix (and its transpose) is returned once the
-    Matrix and its tensor views are dropped."""
+    Matrix and its tensor views are dropped: to the library's block cache,
+    which trim_memory empties."""
     lst = np.arange(0, 60000, dtype=np.int32)
     A = ctx_small.build(lst, 100, SEED)  # warms the context scratch
     del A
     torch.cuda.synchronize()
+    rlib.trim_memory()
     free0 = torch.cuda.mem_get_info()[0]
     A = ctx_small.build(lst, 100, SEED)
     A.transpose()
@@ -504,7 +506,9 @@ def test_matrix_memory_is_released(rlib, torch, ctx_small):
     col_view = A.col[:10]
     del A
     torch.cuda.synchronize()
+    rlib.trim_memory()
     assert torch.cuda.mem_get_info()[0] < free0 - nbytes // 2  # the view keeps it alive
     del col_view
     torch.cuda.synchronize()
+    rlib.trim_memory()
     assert torch.cuda.mem_get_info()[0] > free0 - nbytes // 4
