@@ -147,3 +147,33 @@ def test_freed_blocks_are_reused_and_trimmed(rlib, torch):
     rlib.trim_memory()
     free_trimmed = torch.cuda.mem_get_info()[0]
     assert free_trimmed - free_kept >= 2 * col0.nbytes
+
+
+def test_rows_that_overflow_the_first_table_are_rebuilt(rlib, oracle, torch):
+    # A 25 mm grid of 0.5 mm voxels with 64 rays per channel starts at the
+    # smallest row table (2048 entries); a quarter of the rows hold more
+    # voxels than that, in both of the build's chunks (85,683 rows, 65,536
+    # per chunk), so the build drains its pipeline, rebuilds those chunks at
+    # the next level and carries on.  Rows from both chunks against the
+    # oracle.
+    g = cfg.Geometry(grid_o=(-0.0125,) * 3, grid_d=(0.0005,) * 3, grid_n=(50,) * 3, pos0x=-0.240, pos1x=0.240,
+                     na=3, n0z=13, n0y=13, n1z=13, n1y=13, da=30.0, segx=0.020, segy=0.004, segz=0.004)
+    ctx = rlib.Context(g, 0)
+    lst = np.arange(g.n_channels, dtype=np.int32)
+    A = ctx.build(lst, 64, 1251)
+    rp, col, val = A.to_numpy()
+    lens = np.diff(rp)
+    big = np.nonzero(lens > 2048)[0]
+    assert big.size > 0 and big.min() < 65536 <= big.max()
+    rng = np.random.default_rng(4)
+    pick = np.unique(np.concatenate([rng.choice(big[big < 65536], 10), rng.choice(big[big >= 65536], 10),
+                                     rng.choice(lst.size, 20)]))
+    rp_o, col_o, val_o = oracle.sysmat(g, lst[pick], 64, 1251, method=1)
+    for k, i in enumerate(pick):
+        got_c = col[rp[i]:rp[i + 1]]
+        got_v = val[rp[i]:rp[i + 1]]
+        want_c = col_o[rp_o[k]:rp_o[k + 1]]
+        want_v = val_o[rp_o[k]:rp_o[k + 1]].astype(np.float64)
+        assert np.array_equal(got_c, want_c), f"row {i}"
+        if want_v.size:
+            assert np.max(np.abs(got_v - want_v) / want_v) <= 1e-5, f"row {i}"
