@@ -124,7 +124,6 @@ struct DenseIndex {
   const int* base;
   const int* dk;
   int wv, nslots;
-  int* fail;
   int slot, sa, ka, sta, ku, kv;
   __device__ __forceinline__ void begin(const int step[3]) {
     sta = step[A];
@@ -147,10 +146,9 @@ struct DenseIndex {
     ka = dk[sa];
   }
   __device__ __forceinline__ void add(float L) const {
-    if (unsigned(slot) < unsigned(nslots))
-      atomicAdd(&acc[slot], L);
-    else
-      *fail = 1;
+    // a slot outside the windows goes to the spare slot at nslots, which
+    // the row checks afterwards (no branch in the step loop)
+    atomicAdd(&acc[unsigned(slot) < unsigned(nslots) ? slot : nslots], L);
   }
 };
 
@@ -197,7 +195,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
     if (s[d]) {
       const int n = g.n[d];
       float pos = r[d] + amin_g * dir[d];
-      int i = int(floorf((pos - g.o[d]) / g.d[d]));
+      int i = int(floorf(__fdividef(pos - g.o[d], g.d[d])));  // a guess: corrected below
       i = min(max(i, 0), n - 1);
       // Exact correction against the plane parameters: find the voxel whose
       // interval [lo, hi) contains the entry parameter.
@@ -269,7 +267,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
       const int nD = D == 0 ? g.n[0] : (D == 1 ? g.n[1] : g.n[2]);
       const int iD = D == 0 ? i0 : (D == 1 ? i1 : i2);
       const float hD = D == 0 ? hi0 : (D == 1 ? hi1 : hi2);
-      const int span = int(fabsf((amax_g - amin_g) * dD) / pD) + 1;
+      const int span = int(__fdividef(fabsf((amax_g - amin_g) * dD), pD)) + 1;
       const int k = (part * span) >> 8;
       const int is = iD + stD * k;
       if (k > 0 && is >= 0 && is < nD) {
@@ -286,7 +284,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
               nh[d] = plane_alpha_r(oD, pD, stD > 0 ? is + 1 : is, rD, dD, cD);
             } else {
               // the voxel of axis d whose interval [lo, hi) holds as
-              int i = int(floorf((r[d] + as * dir[d] - g.o[d]) / g.d[d]));
+              int i = int(floorf(__fdividef(r[d] + as * dir[d] - g.o[d], g.d[d])));
               i = min(max(i, 0), g.n[d] - 1);
               float l = 0.f, h = 0.f;
               bool found = false;
@@ -604,7 +602,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
   }
   const int wu = win_u, wv = win_v;
   const int wuv = wu * wv;
-  bool use_dense = A >= 0 && (long long)na * wuv <= (long long)dense_slots(H);
+  bool use_dense = A >= 0 && (long long)na * wuv < (long long)dense_slots(H);  // + the spare slot
   const int nslots = use_dense ? na * wuv : 0;
 
   const float fr = float(nrays);
@@ -633,7 +631,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
         sbase[sl] = b;
         sdk[sl] = bn - b;
       }
-      for (int i = tid; i < nslots; i += T) acc[i] = 0.f;
+      for (int i = tid; i <= nslots; i += T) acc[i] = 0.f;
     } else {
       for (int i = tid; i < H; i += T) {
         keys[i] = -1;
@@ -651,8 +649,8 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
         else
           dense_fail = 1;
       };
-      DenseIndex<0> dix0{acc, sbase, sdk, wv, nslots, &dense_fail};
-      DenseIndex<2> dix2{acc, sbase, sdk, wv, nslots, &dense_fail};
+      DenseIndex<0> dix0{acc, sbase, sdk, wv, nslots};
+      DenseIndex<2> dix2{acc, sbase, sdk, wv, nslots};
       for (int ray = tid; ray < nrays; ray += T) {
         float r[6];
         make_ray(ch, seed, cnl, ray, r);
@@ -683,7 +681,10 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
       }
     }
     __syncthreads();
-    if (use_dense && !dense_fail && !bad_walk) {
+    // a slot outside the windows was added to the spare slot: every thread
+    // reads the same value and takes the same branch
+    const bool spare = use_dense && acc[nslots] != 0.f;
+    if (use_dense && !dense_fail && !bad_walk && !spare) {
       // First compaction pass: per warp, count the voxels with a positive
       // sum that pass the cylinder test and clear the others.  A positive
       // slot that decodes to a voxel outside the grid means the windows
@@ -710,7 +711,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
       if (lane == 0) warp_sums[w] = cnt;
       __syncthreads();
     }
-    if (!(use_dense && dense_fail)) break;
+    if (!(use_dense && (dense_fail || spare))) break;
     use_dense = false;  // redo the row with the table
     __syncthreads();
   }
