@@ -5,7 +5,7 @@
 // order); each pass is a stable partition by the next 10 bits of the column,
 // so after the passes the entries are sorted by (column, k).  A pass is
 // histogram -> scan -> scatter over tiles of ~128K entries, one CTA each:
-// the CTA ranks its entries in chunks of 4096 (32 warps x 4 items x 32
+// the CTA ranks its entries in chunks of 8192 (32 warps x 8 items x 32
 // lanes) with __match_any_sync and per-warp digit counters in shared
 // memory.  In the first pass a chunk is staged in shared memory in sorted
 // order and written out by consecutive threads, so that the stores of a
@@ -31,7 +31,7 @@ namespace {
 constexpr int kRadixBits = 10;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kWarps = 32;
-constexpr int kItems = 4;
+constexpr int kItems = 8;
 constexpr int kChunk = kWarps * kItems * 32;  // entries ranked together
 constexpr int kMaxTileRows = 1024;
 constexpr int64_t kTileEntries = 131072;
