@@ -153,10 +153,12 @@ struct DenseIndex {
 };
 
 // Visits every grid voxel whose intersection length with ray r is positive.
-// emit(ix, iy, iz, L) for the common case of a ray that crosses the planes
-// of all three axes; a ray parallel to the planes of some axis (start and
-// end coordinate equal) leaves that axis unconstrained, as the reference's
-// masked min/max does, and every candidate voxel along it gets the length.
+// A ray that crosses the planes of all three axes takes the step loop,
+// which adds the lengths through the index `ix`; any other ray takes the
+// general loop, which adds through emit(ix, iy, iz, L): a ray parallel to
+// the planes of some axis (start and end coordinate equal) leaves that axis
+// unconstrained, as the reference's masked min/max does, and every
+// candidate voxel along it gets the length.
 template <bool OISO, class Emit, class Index>
 __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, const float r[6], int part, Emit& emit,
                                          Index& ix, int* bad_walk) {
