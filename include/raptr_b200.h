@@ -360,9 +360,11 @@ raptr_status raptr_mlem_batch_autotune(raptr_ctx* ctx, int64_t m, int64_t n, int
  * atomics); the caller passes the matrix, y, s and x (updated in place).
  * The workspace is a fixed device array inside the library, sized for at
  * most 1,048,576 voxels (4 MiB, held on every GPU that loads the library
- * until exit); larger n is rejected with RAPTR_ERR_INVALID.  Runs on the
- * current device; the first call on a device looks up the array's device
- * address, so make that first call before any stream capture.  All calls on
+ * until exit); larger n is rejected with RAPTR_ERR_INVALID, and so are null
+ * d_col / d_val when m > 0.  Runs on the current device; the first call on
+ * a device looks up the array's device address, so make that first call
+ * before any stream capture.  That address is kept for the life of the
+ * process: do not use the library across a cudaDeviceReset.  All calls on
  * a device share the array: each call clears what must start at zero, and
  * calls that overlap on the GPU race on it. */
 raptr_status raptr_mlem_noalloc(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,

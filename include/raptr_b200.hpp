@@ -392,6 +392,7 @@ struct DeviceConstants {
   int nrays = 0;
   uint32_t seed = 1251;
   int device = 0;
+  int32_t sm_flags = 0; /* raptr_sm_build flags of systemMatrixCalculation */
   std::shared_ptr<raptr_ctx> ctx;
 };
 
@@ -413,6 +414,11 @@ inline void set_device_constants(VG const& grid, MS const& setup, int nrays, uin
   check(raptr_ctx_create(&c.geom, c.device, &ctx), "raptr_ctx_create");
   c.ctx = std::shared_ptr<raptr_ctx>(ctx, [](raptr_ctx* p) { raptr_ctx_destroy(p); });
 }
+
+/* Flags for the builds of systemMatrixCalculation on this thread:
+ * RAPTR_SM_KEEP_ZEROS keeps every candidate of a row, exact zeros included,
+ * which is the reference's structure; the default (0) drops exact zeros. */
+inline void set_sm_flags(int32_t flags) { device_constants().sm_flags = flags; }
 
 inline raptr_ctx* current_ctx() {
   DeviceConstants& c = device_constants();
@@ -496,7 +502,9 @@ int getWorkqueue(std::vector<int>& returnCnlId, std::vector<int>& returnVxlId, i
  * voxels); *nnz_devi is increased by the number of entries.  The COO row
  * ids and the CSR over all channels are internal to the reference's
  * pipeline and are not produced (aCnlId_devi, aCsrCnlPtr_devi untouched).
- * Geometry and ray count come from raptr::set_device_constants. */
+ * Geometry and ray count come from raptr::set_device_constants.  Exact
+ * zeros are dropped unless raptr::set_sm_flags(RAPTR_SM_KEEP_ZEROS) was
+ * called: then every candidate is kept, as the reference stores them. */
 template <typename T, typename ListSizeType, typename GridSizeType, typename MemArrSizeType, typename RayGen,
           typename Handle>
 void systemMatrixCalculation(int* const aEcsrCnlPtr_devi, GridSizeType* const aVxlId_devi, T* const aVal_devi,
@@ -513,7 +521,7 @@ void systemMatrixCalculation(int* const aEcsrCnlPtr_devi, GridSizeType* const aV
   const int64_t nvox = int64_t(c.geom.grid_n[0]) * c.geom.grid_n[1] * c.geom.grid_n[2];
   raptr::DeviceBuffer<int64_t> rp(size_t(m + 1));
   int64_t nnz = 0;
-  raptr::check(raptr_sm_build(ctx, yRowId_devi, m, c.nrays, c.seed, nullptr, 0, m * nvox, rp.p,
+  raptr::check(raptr_sm_build(ctx, yRowId_devi, m, c.nrays, c.seed, nullptr, c.sm_flags, m * nvox, rp.p,
                               reinterpret_cast<int32_t*>(aVxlId_devi), aVal_devi, &nnz, nullptr),
                "raptr_sm_build");
   raptr::check(raptr_row_ptr_narrow(rp.p, m + 1, aEcsrCnlPtr_devi, nullptr), "raptr_row_ptr_narrow");

@@ -823,17 +823,81 @@ void ora_column_sums_f64(int64_t m, int64_t n, const int64_t* rp, const int32_t*
     for (int64_t k = rp[i]; k < rp[i + 1]; k++) s[col[k]] += double(val[k]);
 }
 
+}  // extern "C"
+
+namespace {
+
+/* The transposed operand of the oracle's MLEM: for every column its rows in
+ * ascending order with their values.  Summing a column's products in that
+ * order adds them exactly as the sequential scatter y[col[k]] += a*x[i]
+ * over rows i = 0, 1, ... does, so the back projection below is the same,
+ * bit for bit, as spmv_t(1, ...) while its columns run in parallel. */
+struct Csc {
+  std::vector<int64_t> cp;
+  std::vector<int32_t> row;
+  std::vector<float> val;
+};
+
+Csc csc_of(int64_t m, int64_t n, const int64_t* rp, const int32_t* col, const float* val) {
+  Csc t;
+  const int64_t nnz = rp[m];
+  t.cp.assign(size_t(n) + 1, 0);
+  for (int64_t k = 0; k < nnz; k++) t.cp[size_t(col[k]) + 1]++;
+  for (int64_t j = 0; j < n; j++) t.cp[size_t(j) + 1] += t.cp[size_t(j)];
+  t.row.resize(size_t(nnz));
+  t.val.resize(size_t(nnz));
+  std::vector<int64_t> next(t.cp.begin(), t.cp.end() - 1);
+  for (int64_t i = 0; i < m; i++)
+    for (int64_t k = rp[i]; k < rp[i + 1]; k++) {
+      const int64_t p = next[size_t(col[k])]++;
+      t.row[size_t(p)] = int32_t(i);
+      t.val[size_t(p)] = val[k];
+    }
+  return t;
+}
+
+/* y = A x (op N, one row at a time, in entry order) and c = A^T e (op T,
+ * one column at a time, in row order): the sums of spmv_t with alpha 1 and
+ * beta 0, in the same order, rows / columns in parallel. */
+template <typename T>
+void forward_rows(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const T* x, T* y) {
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < m; i++) {
+    T s = 0;
+    for (int64_t k = rp[i]; k < rp[i + 1]; k++) s += T(val[k]) * x[col[k]];
+    y[i] = T(1) * s;
+  }
+}
+
+template <typename T>
+void back_columns(int64_t n, const Csc& t, const T* e, T* c) {
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t j = 0; j < n; j++) {
+    T s = 0;
+    for (int64_t p = t.cp[size_t(j)]; p < t.cp[size_t(j) + 1]; p++) s += T(1) * T(t.val[size_t(p)]) * e[t.row[size_t(p)]];
+    c[j] = s;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
 /* MLEM iterations in the order of src/tests/reco.cu:230-303 (single rank,
  * one chunk): c = 0; yt = A x; e = y / yt; c = A^T e; xx = x*c/(s + (s==0));
  * x = xx; x *= 1/sum(x).  `s` must already be normalised.  FP32 version
- * uses float vectors, FP64 version double vectors (same matrix values). */
+ * uses float vectors, FP64 version double vectors (same matrix values).
+ * Every sum is taken in the order of the sequential CSRmv restatement
+ * spmv_t (rows in entry order; columns in row order), so the result does
+ * not depend on the thread count. */
 void ora_mlem_f32(int64_t m, int64_t n, const int64_t* rp, const int32_t* col, const float* val, const float* y,
                   const float* s, float* x, int32_t niter) {
   std::vector<float> yt(m), e(m), c(n), xx(n);
+  const Csc t = csc_of(m, n, rp, col, val);
   for (int32_t it = 0; it < niter; it++) {
-    spmv_t<float>(0, m, n, rp, col, val, 1.f, x, 0.f, yt.data());
+    forward_rows<float>(m, rp, col, val, x, yt.data());
     for (int64_t i = 0; i < m; i++) e[i] = y[i] / yt[i];
-    spmv_t<float>(1, m, n, rp, col, val, 1.f, e.data(), 0.f, c.data());
+    back_columns<float>(n, t, e.data(), c.data());
     ora_divides_multiplies(xx.data(), x, c.data(), s, n);
     std::copy(xx.begin(), xx.end(), x);
     double norm = 0.0;
@@ -846,10 +910,11 @@ void ora_mlem_f32(int64_t m, int64_t n, const int64_t* rp, const int32_t* col, c
 void ora_mlem_f64(int64_t m, int64_t n, const int64_t* rp, const int32_t* col, const float* val, const double* y,
                   const double* s, double* x, int32_t niter) {
   std::vector<double> yt(m), e(m), c(n);
+  const Csc t = csc_of(m, n, rp, col, val);
   for (int32_t it = 0; it < niter; it++) {
-    spmv_t<double>(0, m, n, rp, col, val, 1.0, x, 0.0, yt.data());
+    forward_rows<double>(m, rp, col, val, x, yt.data());
     for (int64_t i = 0; i < m; i++) e[i] = y[i] / yt[i];
-    spmv_t<double>(1, m, n, rp, col, val, 1.0, e.data(), 0.0, c.data());
+    back_columns<double>(n, t, e.data(), c.data());
     for (int64_t j = 0; j < n; j++) {
       double dvs = s[j];
       dvs += double(dvs == 0.);

@@ -86,33 +86,53 @@ cudaError_t dev_alloc(void** p, size_t bytes) {
 
 void dev_free(void* p) {
   if (!p) return;
-  std::unique_lock<std::mutex> lock(g_mu);
-  auto it = g_live.find(p);
-  if (it == g_live.end()) {
-    lock.unlock();
+  Block b{};
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto it = g_live.find(p);
+    if (it != g_live.end()) {
+      b = it->second;
+      g_live.erase(it);
+    }
+  }
+  if (b.bytes == 0) {
     cudaFree(p);
     return;
   }
-  const Block b = it->second;
-  g_live.erase(it);
-  size_t total = 0, freeb = 0;
   int cur = -1;
   cudaGetDevice(&cur);
   if (cur != b.device) cudaSetDevice(b.device);
-  // like cudaFree, wait for the device's work (which may still use the
-  // block) before the block can be handed out again
-  bool info = cudaDeviceSynchronize() == cudaSuccess;
-  if (info && !g_total.count(b.device)) {
-    info = cudaMemGetInfo(&freeb, &total) == cudaSuccess;
-    if (info) g_total[b.device] = total;
+  // Like cudaFree, wait for the device's work (which may still use the
+  // block) before the block can be handed out again.  The wait runs without
+  // the lock, so that other threads' allocations do not wait for it too.
+  bool ok = cudaDeviceSynchronize() == cudaSuccess;
+  size_t total = 0, freeb = 0;
+  bool park = false;
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (ok && !g_total.count(b.device)) {
+      ok = cudaMemGetInfo(&freeb, &total) == cudaSuccess;
+      if (ok) g_total[b.device] = total;
+    }
+    if (ok) {
+      total = g_total[b.device];
+      park = g_parked_bytes[b.device] + b.bytes <= total / 2;
+      if (park) {
+        g_parked[b.device].emplace(b.bytes, p);
+        g_parked_bytes[b.device] += b.bytes;
+      }
+    }
   }
-  if (info) total = g_total[b.device];
-  if (info && g_parked_bytes[b.device] + b.bytes <= total / 2) {
-    g_parked[b.device].emplace(b.bytes, p);
-    g_parked_bytes[b.device] += b.bytes;
-  } else {
+  if (!park) {
+    // a failed wait (a stream being captured, a device error) leaves the
+    // block's use unknown: hand it back to the driver, never to the cache
     (void)cudaGetLastError();
-    cudaFree(p);
+    const cudaError_t e = cudaFree(p);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      trace("dev_free: cudaFree of a %zu-byte block failed (%s); the block is leaked", b.bytes,
+            cudaGetErrorString(e));
+    }
   }
   if (cur >= 0 && cur != b.device) cudaSetDevice(cur);
 }

@@ -91,4 +91,24 @@ class LruBudget {
   std::map<Key, typename std::list<Node>::iterator> index_;
 };
 
+// Admission of a request whose matrix is not resident: `need` bytes (the
+// matrix estimate plus the request's state) on top of what is in use.
+//   kAdmit: fits after evicting `victims` (possibly none);
+//   kWait:  cannot fit while other work holds memory -- retry later;
+//   kFail:  cannot fit even with every unpinned entry evicted and nothing
+//           else running -- fail it, and evict nothing.
+enum class Admission { kAdmit, kWait, kFail };
+
+template <class Key>
+Admission decide_admission(const LruBudget<Key>& cache, int64_t need, bool running, std::vector<Key>* victims) {
+  bool fits = false;
+  std::vector<Key> v = cache.victims(need, &fits);
+  victims->clear();
+  if (fits) {
+    *victims = std::move(v);
+    return Admission::kAdmit;
+  }
+  return running ? Admission::kWait : Admission::kFail;
+}
+
 }  // namespace raptr

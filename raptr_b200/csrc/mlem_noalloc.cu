@@ -37,7 +37,10 @@ std::mutex g_mu;
 void* g_addr[kMaxDevices] = {};
 
 // Device address of the array on the current device, looked up once per
-// device (host code cannot use the symbol itself as a device pointer).
+// device (host code cannot use the symbol itself as a device pointer).  The
+// address belongs to the device's primary context: after cudaDeviceReset
+// the library's device state (this address, contexts, cached blocks) is
+// gone, so the library must not be used across a reset.
 cudaError_t scratch_address(int dev, void** out) {
   std::lock_guard<std::mutex> lock(g_mu);
   if (!g_addr[dev]) {
@@ -58,7 +61,12 @@ raptr_status mlem_noalloc(int64_t m, int64_t n, const int64_t* rp, const int32_t
                           const float* y, const float* s, float* x, int32_t n_iter, cudaStream_t st,
                           std::string* err) {
   if (m < 0 || n <= 0 || n_iter < 0 || !rp || !y || !s || !x) {
-    *err = "bad argument";
+    *err = "raptr_mlem_noalloc: bad argument";
+    return RAPTR_ERR_INVALID;
+  }
+  if (m > 0 && (!col || !val)) {
+    // the row pointers alone cannot tell whether the rows hold entries
+    *err = "raptr_mlem_noalloc: null column or value array for a matrix with rows";
     return RAPTR_ERR_INVALID;
   }
   if (n > kMaxVoxels) {

@@ -342,20 +342,19 @@ bool raptr_server::admit(std::unique_lock<std::mutex>& lk) {
     const int64_t state_need = voxels_of(r->g) * 4 + channels_of(r->g) * 4 * 3;  // y + batch growth
     if (!e) {
       const int64_t est = cache.contains(r->key) ? cache.bytes(r->key) : estimate_bytes(r->g);
-      bool fits = false;
-      std::vector<std::string> victims = cache.victims(est + state_bytes + state_need, &fits);
-      if (!fits) {
-        // wait for running work to finish; fail only when nothing runs
-        bool running = false;
-        for (auto& kv : entries) running = running || !kv.second->active.empty();
-        if (running) break;
-        if (cache.used() == 0 || victims.empty()) {
-          fail_request(r, RAPTR_ERR_NOMEM, "the matrix does not fit the HBM budget");
-          it = queue.erase(it);
-          cv_done.notify_all();
-          changed = true;
-          continue;
-        }
+      bool running = false;
+      for (auto& kv : entries) running = running || !kv.second->active.empty();
+      std::vector<std::string> victims;
+      const Admission adm = decide_admission(cache, est + state_bytes + state_need, running, &victims);
+      // wait for running work to finish; fail (evicting nothing) when the
+      // request cannot fit even with nothing else resident
+      if (adm == Admission::kWait) break;
+      if (adm == Admission::kFail) {
+        fail_request(r, RAPTR_ERR_NOMEM, "the matrix does not fit the HBM budget");
+        it = queue.erase(it);
+        cv_done.notify_all();
+        changed = true;
+        continue;
       }
       for (auto& v : victims) {
         auto vi = entries.find(v);

@@ -51,6 +51,24 @@ int main() {
   CHECK(c.used() == 80 && !c.contains("a"));
   v = c.victims(0, &fits);
   CHECK(fits && v.empty());
+
+  // admission: an oversized request fails without evicting idle entries
+  raptr::LruBudget<std::string> d(100);
+  d.put("idle", 60);
+  std::vector<std::string> vic;
+  CHECK(raptr::decide_admission(d, 120, false, &vic) == raptr::Admission::kFail && vic.empty());
+  CHECK(d.contains("idle") && d.used() == 60);
+  // ... and waits while other work runs
+  CHECK(raptr::decide_admission(d, 120, true, &vic) == raptr::Admission::kWait && vic.empty());
+  // a request that fits after evicting the idle entry is admitted
+  CHECK(raptr::decide_admission(d, 70, false, &vic) == raptr::Admission::kAdmit && vic.size() == 1 &&
+        vic[0] == "idle");
+  // one that fits as is evicts nothing
+  CHECK(raptr::decide_admission(d, 40, false, &vic) == raptr::Admission::kAdmit && vic.empty());
+  // a pinned entry in the way: wait if work runs, else fail
+  d.pin("idle");
+  CHECK(raptr::decide_admission(d, 70, true, &vic) == raptr::Admission::kWait);
+  CHECK(raptr::decide_admission(d, 70, false, &vic) == raptr::Admission::kFail && vic.empty());
   std::printf("failures %d\n", failures);
   return failures == 0 ? 0 : 1;
 }

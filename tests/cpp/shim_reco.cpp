@@ -1,8 +1,10 @@
 // The reference's reco iteration (src/tests/reco.cu:230-303) written against
 // the C++ template API of include/raptr_b200.hpp: systemMatrixCalculation,
 // CSRmv<float>, divides, dividesMultiplies, sum, scales.  Small geometry,
-// every 301st channel, 5 iterations; writes the image to argv[1].
+// every 301st channel, 5 iterations; writes the image to argv[1].  With
+// argv[2] = "keep" the rows keep exact zeros (the reference's structure).
 #include <cstdio>
+#include <string>
 #include <vector>
 
 #include "raptr_b200.hpp"
@@ -14,12 +16,13 @@ typedef DefaultMeasurementSetup<val_t> MS;
 #define CK(x) raptr::check_cuda((x), #x)
 
 int main(int argc, char** argv) {
-  if (argc != 2) return 2;
+  if (argc < 2 || argc > 3) return 2;
   try {
     VG grid(-0.04f, -0.04f, -0.04f, 0.002f, 0.002f, 0.002f, 40, 40, 40);
     MS setup(-0.24f, 0.24f, 5, 13, 13, 13, 13, 36.f, 0.020f, 0.004f, 0.004f);
     const int nrays = 100;
     raptr::set_device_constants(grid, setup, nrays, 1251);
+    if (argc == 3 && std::string(argv[2]) == "keep") raptr::set_sm_flags(RAPTR_SM_KEEP_ZEROS);
     const int M = 5 * 13 * 13 * 13 * 13, N = 40 * 40 * 40;
     std::vector<int> yRowId;
     for (int c = 0; c < M; c += 301) yRowId.push_back(c);

@@ -43,16 +43,21 @@ def test_shim_host_traits(rlib, oracle, tmp_path):
 
 
 @pytest.mark.gpu
-def test_shim_reco_loop_on_gpu(rlib, oracle, tmp_path):
+@pytest.mark.parametrize("keep_zeros", [False, True])
+def test_shim_reco_loop_on_gpu(rlib, oracle, tmp_path, keep_zeros):
     exe = compile_cpp("shim_reco.cpp", tmp_path)
     out = tmp_path / "x.bin"
-    r = subprocess.run([exe, str(out)], capture_output=True, text=True, timeout=600)
+    r = subprocess.run([exe, str(out)] + (["keep"] if keep_zeros else []), capture_output=True, text=True,
+                       timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     x = np.fromfile(out, np.float32)
     # the same loop on the oracle: rows of the listed channels, y = 1e4 * A x_true
     g = cfg.SMALL
     lst = np.arange(0, g.n_channels, 301, dtype=np.int32)
-    rp, col, val = oracle.sysmat(g, lst, 100, 1251, method=1)
+    rp, col, val = oracle.sysmat(g, lst, 100, 1251, method=1, keep_zeros=keep_zeros)
+    # the entry count the shim added to *nnz_devi: every candidate with
+    # RAPTR_SM_KEEP_ZEROS (the reference's structure), else the non-zeros
+    assert f"rows {lst.size} nnz {int(rp[-1])}" in r.stdout
     xt = cfg.phantom(g, rods=False)
     y = (oracle.spmv(0, lst.size, g.n_voxels, rp, col, val, xt) * 1e4).astype(np.float32)
     s = oracle.column_sums_f64(lst.size, g.n_voxels, rp, col, val)

@@ -1,6 +1,10 @@
 """Batched frames on the GPU: K reconstructions over one matrix in one
 multi-right-hand-side pass must give, frame by frame, the single-frame
-iteration's image (same matrix form), for every frame tile."""
+iteration's image (same matrix form), for every frame tile.  At 64 frames
+of uneven counts (the dynamic-PET form: one geometry, counts log-uniform
+in [1e5, 1e8]) every tile the autotuner can pick is checked, in FP32 and
+FP16, against the single-frame iteration and against the CPU FP64 oracle
+(src/tests/reco.cu:229-321 in FP64 over the measured rows)."""
 import numpy as np
 import pytest
 
@@ -11,6 +15,9 @@ pytestmark = pytest.mark.gpu
 SEED = 1251
 K = 8
 FRAME_RTOL = 1e-5  # batched vs single-frame image (relative L2); summation order differs
+F64_RTOL = {False: 1e-4, True: 1e-3}  # vs the FP64 oracle: FP32 matrix, FP16 matrix
+K64 = 64
+NIT64 = 6
 
 
 @pytest.fixture(scope="module")
@@ -87,3 +94,97 @@ def test_batch_rejects_bad_tile(rlib, torch, frames):
         ctx.mlem_batch(A, torch.from_numpy(Y).cuda(), s, X, 1, frame_tile=16)  # does not divide 8
     with pytest.raises(RuntimeError):
         ctx.mlem_batch(A, torch.from_numpy(Y).cuda(), s, X, 1, frame_tile=6)
+
+
+# ---------------------------------------------------------------- 64 frames
+
+
+@pytest.fixture(scope="module")
+def frames64(rlib, torch):
+    """64 frames of the C1 geometry: x_true under a seeded exponential
+    washout (rate uniform in [0.01, 0.1] per frame), counts log-uniform in
+    [1e5, 1e8]."""
+    g = cfg.SMALL
+    ctx = rlib.Context(g, 0)
+    A = ctx.build(np.arange(g.n_channels, dtype=np.int32), 100, SEED)
+    A.to_half()
+    rp, col, val = A.to_numpy()
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(64)
+    rate = rng.uniform(0.01, 0.1)
+    xt = cfg.phantom(g, rods=False).astype(np.float64)
+    lam = O.spmv(0, A.m, A.n, rp, col, val, xt, dtype=np.float64)
+    Y = np.zeros((A.m, K64), np.float32)
+    for f in range(K64):
+        counts = 10 ** rng.uniform(5, 8)
+        Y[:, f] = cfg.poisson_measurement(lam * np.exp(-rate * f), counts, seed=1000 + f)
+    return ctx, A, Y, (rp, col, val)
+
+
+@pytest.fixture(scope="module")
+def single64(rlib, torch, frames64):
+    """Single-frame images of all 64 frames, FP32 and FP16 matrix."""
+    ctx, A, Y, _ = frames64
+    n = A.n
+    out = {}
+    for half in (False, True):
+        s = (rlib.sensitivity_half(A) if half else rlib.sensitivity(A))[1]
+        imgs = np.zeros((n, K64), np.float32)
+        for f in range(K64):
+            x = torch.full((n,), np.float32(1.0 / n), device="cuda")
+            y = torch.from_numpy(np.ascontiguousarray(Y[:, f])).cuda()
+            (ctx.mlem_half if half else ctx.mlem)(A, y, s, x, NIT64)
+            imgs[:, f] = x.cpu().numpy()
+        out[half] = imgs
+    return out
+
+
+@pytest.fixture(scope="module")
+def oracle64(frames64):
+    """FP64 oracle images of frames 0, 31 and 63 over their measured rows,
+    with the FP64 sensitivity of all rows."""
+    from oracle import oracle as O
+
+    ctx, A, Y, (rp, col, val) = frames64
+    s = O.column_sums_f64(A.m, A.n, rp, col, val)
+    s /= s.sum()
+    out = {}
+    for f in (0, 31, K64 - 1):
+        rows = np.nonzero(Y[:, f])[0]
+        rp_m = np.concatenate([[0], np.cumsum(np.diff(rp)[rows])]).astype(np.int64)
+        sel = np.concatenate([np.arange(rp[r], rp[r + 1]) for r in rows])
+        x0 = np.full(A.n, 1.0 / A.n)
+        out[f] = O.mlem(rows.size, A.n, rp_m, col[sel], val[sel], Y[rows, f].astype(np.float64), s, x0, NIT64,
+                        dtype=np.float64)
+    return out
+
+
+@pytest.mark.parametrize("half", [False, True])
+@pytest.mark.parametrize("tile", [4, 8, 16, 32, 64])
+def test_batch64_every_tile(rlib, torch, frames64, single64, oracle64, half, tile):
+    ctx, A, Y, _ = frames64
+    n = A.n
+    s = (rlib.sensitivity_half(A) if half else rlib.sensitivity(A))[1]
+    X = torch.full((n, K64), np.float32(1.0 / n), device="cuda")
+    ctx.mlem_batch(A, torch.from_numpy(Y).cuda(), s, X, NIT64, frame_tile=tile, half=half, use_graph=True)
+    Xb = X.cpu().numpy()
+    ref = single64[half]
+    for f in range(K64):
+        err = np.linalg.norm(Xb[:, f] - ref[:, f]) / np.linalg.norm(ref[:, f])
+        assert err < FRAME_RTOL, f"frame {f}: rel L2 {err:.2e} against the single-frame iteration"
+        assert abs(float(Xb[:, f].sum()) - 1.0) < 1e-5
+    for f, want in oracle64.items():
+        err = np.linalg.norm(Xb[:, f].astype(np.float64) - want) / np.linalg.norm(want)
+        assert err < F64_RTOL[half], f"frame {f}: rel L2 {err:.2e} against the FP64 oracle"
+
+
+def test_batch64_autotune_covers_every_tile(rlib, torch, frames64):
+    ctx, A, Y, _ = frames64
+    n = A.n
+    s = rlib.sensitivity_half(A)[1]
+    X0 = torch.full((n, K64), np.float32(1.0 / n), device="cuda")
+    best, ms = ctx.batch_autotune(A, torch.from_numpy(Y).cuda(), s, X0)
+    assert set(ms) == {4, 8, 16, 32, 64} and best in ms
+    assert all(v > 0 for v in ms.values())
+    assert torch.all(X0 == np.float32(1.0 / n))

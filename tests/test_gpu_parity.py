@@ -336,6 +336,46 @@ def test_mlem_matches_oracle(rlib, oracle, torch, ctx_small, small_full_matrix, 
         assert np.all(np.diff(ll) >= -1e-6 * abs(ll[-1]))  # MLEM never decreases the likelihood
 
 
+def test_mlem_full_geometry_four_angles_50_iterations(rlib, oracle, torch, ctx_full):
+    """The full workload's iteration on a row subset of its geometry: all
+    channels of four angles (0, 46, 90 and 134 degrees: x-slab, diagonal and
+    z-slab rows) of the 70^3 grid, 1000 rays, rod phantom, 50 iterations
+    through the transpose in back-projection order (the benchmarked path),
+    against the FP32 and FP64 oracles (src/tests/reco.cu:229-321) at 1e-4
+    relative L2.  A row sample is first checked against the oracle's own
+    rows."""
+    g = cfg.FULL
+    per = g.n0z * g.n0y * g.n1z * g.n1y
+    lst = np.concatenate([np.arange(a * per, (a + 1) * per) for a in (0, 23, 45, 67)]).astype(np.int32)
+    A = ctx_full.build(lst, 1000, SEED)
+    rp, col, val = A.to_numpy()
+    sample = np.arange(0, lst.size, lst.size // 16)
+    rp_o, col_o, val_o = oracle.sysmat(g, lst[sample], 1000, SEED, method=1)
+    rp_s = np.concatenate([[0], np.cumsum(np.diff(rp)[sample])]).astype(np.int64)
+    sel = np.concatenate([np.arange(rp[r], rp[r + 1]) for r in sample])
+    assert_rows_equal(rp_s, col[sel], val[sel], rp_o, col_o, val_o)
+    xt = cfg.phantom(g, rods=True).astype(np.float64)
+    lam = oracle.spmv(0, A.m, A.n, rp, col, val, xt, dtype=np.float64)
+    y = cfg.poisson_measurement(lam, 1e8 * lst.size / g.n_channels, seed=70)
+    rows = np.nonzero(y)[0]
+    rp_m = np.concatenate([[0], np.cumsum(np.diff(rp)[rows])]).astype(np.int64)
+    sel = np.concatenate([np.arange(rp[r], rp[r + 1]) for r in rows])
+    col_m, val_m = col[sel], val[sel]
+    s_all = oracle.column_sums_f64(A.m, A.n, rp, col, val)
+    s = (s_all / s_all.sum()).astype(np.float32)
+    x0 = np.full(A.n, np.float32(1.0 / A.n), np.float32)
+    want32 = oracle.mlem(rows.size, A.n, rp_m, col_m, val_m, y[rows], s, x0, 50)
+    want64 = oracle.mlem(rows.size, A.n, rp_m, col_m, val_m, y[rows].astype(np.float64), s.astype(np.float64),
+                         x0.astype(np.float64), 50, dtype=np.float64)
+    A.transpose()
+    x = torch.from_numpy(x0.copy()).cuda()
+    ctx_full.mlem(A, torch.from_numpy(y).cuda(), torch.from_numpy(s).cuda(), x, 50, use_graph=True)
+    x = x.cpu().numpy()
+    assert np.linalg.norm(x - want32) / np.linalg.norm(want32) < IMG_RTOL
+    assert np.linalg.norm(x - want64) / np.linalg.norm(want64) < IMG_RTOL
+    assert abs(float(x.sum()) - 1.0) < 1e-5
+
+
 def channel_order_keys(g, cnl):
     """Back-projection order key of channels: (angle, z0+z1, y0+y1, z0-z1,
     y0-y1), y1 fastest in the channel id."""

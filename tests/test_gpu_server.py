@@ -121,3 +121,49 @@ def test_budget_too_small_and_timeout(rlib, torch, jobs):
     with pytest.raises(ValueError):
         srv.submit(g, y[:-1], 3, NRAYS, SEED)
     srv.close()
+
+
+def test_many_requests_join_and_leave(rlib, torch):
+    """50 requests of one geometry: 40 submitted at once (batches above 32
+    frames), 10 more while those run (they join the running batch).  Every
+    result equals the same request run alone on the same server (same cached
+    matrix) to 1e-5, and the single-frame FP16 iteration on a matrix built
+    apart to 1e-4 (the two builds' values differ in their last bits, which
+    60-120 iterations carry further than the 1e-5 of a few iterations)."""
+    g = MINI
+    ctx = rlib.Context(g, 0)
+    A = ctx.build(np.arange(g.n_channels, dtype=np.int32), NRAYS, SEED)
+    xt = torch.from_numpy(cfg.phantom(g, rods=False)).cuda()
+    lam = rlib.spmv(rlib.OP_N, A.m, A.n, A.row_ptr, A.col, A.val, xt).cpu().numpy()
+    rng = np.random.default_rng(50)
+    reqs = []
+    for i in range(50):
+        it = int(rng.integers(60, 120)) if i < 40 else int(rng.integers(3, 12))
+        if i == 0:
+            it = 2  # finishes first: the cue for the second wave
+        reqs.append((it, cfg.poisson_measurement(lam, 10 ** rng.uniform(5, 7), 500 + i)))
+    A.to_half()
+    h32 = rlib.sensitivity_half(A)[1]
+    want = []
+    for it, y in reqs:
+        x = torch.full((A.n,), np.float32(1.0 / A.n), device="cuda")
+        ctx.mlem_half(A, torch.from_numpy(y).cuda(), h32, x, it)
+        want.append(x.double().cpu().numpy())
+    srv = rlib.Server(0, hbm_budget_bytes=20 << 30)
+    ids = [srv.submit(g, y, it, NRAYS, SEED) for it, y in reqs[:40]]
+    x0, st0 = srv.wait(ids[0], g.n_voxels)
+    running_before = srv.stats()["running"]
+    ids += [srv.submit(g, y, it, NRAYS, SEED) for it, y in reqs[40:]]
+    out = [(x0, st0)] + [srv.wait(rid, g.n_voxels) for rid in ids[1:]]
+    assert running_before > 0  # the second wave arrived while the first ran
+    alone = [srv.wait(srv.submit(g, y, it, NRAYS, SEED), g.n_voxels) for it, y in reqs]
+    srv.close()
+    frames = []
+    for (it, _), w, (x, st), (xa, sta) in zip(reqs, want, out, alone):
+        assert st["iterations"] == it and sta["iterations"] == it and sta["frames_max"] == 1
+        assert rel(x, xa.astype(np.float64)) < MIX_RTOL
+        assert rel(x, w) < 1e-4
+        assert abs(float(x.sum()) - 1.0) < 1e-5
+        frames.append(st["frames_max"])
+    assert max(frames[:40]) > 32  # batches above 32 frames ran
+    assert min(frames[40:]) > 1   # the late requests ran beside others
