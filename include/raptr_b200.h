@@ -24,6 +24,7 @@
  *   raptr_scales           scales                  src/mlemOperations.hpp:146-153
  *   raptr_sum              sum                     src/mlemOperations.hpp:163-169
  *   raptr_mlem             MLEM loop               src/tests/reco.cu:229-321
+ *   raptr_mlem_stream      chunked MLEM loop       src/tests/reco.cu:226-275, src/wrappers.hpp:429-464
  *   raptr_reco_host        reco main flow          src/tests/reco.cu:53-352
  */
 #ifndef RAPTR_B200_H
@@ -35,7 +36,7 @@
 extern "C" {
 #endif
 
-#define RAPTR_ABI_VERSION 3
+#define RAPTR_ABI_VERSION 4
 
 typedef enum raptr_status {
   RAPTR_OK = 0,
@@ -330,9 +331,10 @@ raptr_status raptr_mlem_f64(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t*
  * d_tval float) or the FP16 form (value_type 1: d_val = hval, d_tval =
  * htval, d_rscale the row scales); the transpose is required and d_row_rank
  * follows it (raptr_matrix_row_order, may be null for the natural order).
- * Each pass handles frame_tile frames per sweep of the matrix (4, 8, 16, 32
- * or 64, dividing n_frames; 0 = the default 32-or-smaller divisor); d_x
- * must be 16-byte aligned.
+ * n_frames must be a multiple of 4.  Each pass handles up to frame_tile
+ * frames per sweep of the matrix (4, 8, 16, 32 or 64; 0 = 32): tiles of
+ * frame_tile frames while that many remain, then the largest power of two
+ * that fits (40 frames at 32: 32 + 8).  d_x must be 16-byte aligned.
  * opts: use_graph captures the n_iter iterations in a CUDA graph;
  * h_kernel_ms receives per iteration the forward and back-pass times. */
 raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_frames, int32_t value_type,
@@ -343,13 +345,43 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
                               void* stream);
 /* Picks the frame tile by timing one iteration per candidate on a copy of
  * d_x (left unchanged): *best_tile, and h_ms[5] (when non-null) the times
- * for tiles 4, 8, 16, 32, 64 (-1 where the tile does not divide n_frames). */
+ * for tiles 4, 8, 16, 32, 64 (n_frames a multiple of 4). */
 raptr_status raptr_mlem_batch_autotune(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_frames, int32_t value_type,
                                        const int64_t* d_row_ptr, const int32_t* d_col, const void* d_val,
                                        const float* d_rscale, const int64_t* d_col_ptr, const int32_t* d_row_idx,
                                        const void* d_tval, const int32_t* d_row_rank, const float* d_y,
                                        const float* d_s, const float* d_x, int32_t* best_tile, float* h_ms,
                                        void* stream);
+
+/* ---- MLEM with rows rebuilt in every iteration ------------------------------
+ * Replaces the reference's chunked reconstruction (src/tests/reco.cu:226-275:
+ * per iteration and per chunk of LIMM measured rows, getSystemMatrix ->
+ * cooSort -> coo2csr -> forward CSRmv -> divides -> transposed CSRmv; chunk
+ * sizes src/wrappers.hpp:429-464), which bounds memory by rebuilding the
+ * matrix chunk by chunk, for problems whose system matrix does not fit the
+ * device.  The rows of the listed channels are built in chunks; after the
+ * first iteration the leading rows that fit resident_bytes (CSR at 8 bytes
+ * per entry plus 8 per row) stay resident, and the other rows are rebuilt,
+ * forward-projected and back-projected (scattered) in every iteration
+ * straight from the build's staging, never stored.  d_y: counts of the
+ * listed channels (rows with y == 0 are not projected).  d_s: the
+ * normalised sensitivity, or null to compute it in the first iteration
+ * (FP64 column sums of every listed row, normalised to sum 1); d_s_out
+ * (optional, num_voxels floats) receives the one used.  d_x (num_voxels)
+ * is updated in place.  Besides resident_bytes the call uses about 1 GiB of
+ * row staging and a few image-sized vectors; resident_bytes = 0 rebuilds
+ * every row in every iteration, as the reference does.  Synchronises. */
+typedef struct raptr_stream_stats {
+  int64_t resident_rows;    /* leading rows kept after the first iteration  */
+  int64_t resident_entries; /* their entries                                 */
+  int64_t streamed_rows;    /* rows rebuilt in every iteration               */
+  int32_t level;            /* row table level the rows were built at        */
+  double first_iter_ms;     /* first iteration: every row built              */
+  double iter_ms;           /* mean of the later iterations                  */
+} raptr_stream_stats;
+raptr_status raptr_mlem_stream(raptr_ctx* ctx, const int32_t* d_cnl, int64_t n_list, int32_t nrays, uint32_t seed,
+                               const float* d_y, const float* d_s, float* d_s_out, float* d_x, int32_t n_iter,
+                               int64_t resident_bytes, raptr_stream_stats* stats, void* stream);
 
 /* MLEM iterations that allocate no device memory.  No counterpart in the
  * reference (which allocates its buffers itself).  For callers that cannot
@@ -423,12 +455,19 @@ raptr_status raptr_server_get_stats(raptr_server* s, raptr_server_stats* out);
 
 typedef struct raptr_reco_stats {
   double build_ms;      /* system matrix build (all channels)            */
-  double sens_ms;       /* sensitivity                                   */
+  double sens_ms;       /* sensitivity, normalisation, start image       */
   double iter_ms;       /* all MLEM iterations                           */
-  double total_ms;      /* whole call including copies                   */
-  int64_t nnz;          /* entries of the matrix                         */
+  double total_ms;      /* device time from the first copy to the image  */
+  int64_t nnz;          /* entries of the matrix (resident ones if streamed) */
   int64_t h2d_bytes;    /* bytes copied host -> device                   */
   int64_t d2h_bytes;    /* bytes copied device -> host                   */
+  double transpose_ms;  /* transpose in back-projection order            */
+  double inputs_ms;     /* allocations and copy of the counts            */
+  double output_ms;     /* copy of the image to the host                 */
+  double setup_ms;      /* host time creating the context and stream     */
+  double release_ms;    /* host time returning the device memory         */
+  double wall_ms;       /* host time of the whole call                   */
+  int64_t streamed_rows;/* rows rebuilt in every iteration (0: resident) */
 } raptr_reco_stats;
 
 /* The reco executable's flow from host buffers (src/tests/reco.cu:53-352):
@@ -437,7 +476,10 @@ typedef struct raptr_reco_stats {
  * from h_x0 (num_voxels floats; null = uniform image normalised to sum 1),
  * result in h_x (num_voxels floats).  The sensitivity is computed from the
  * matrix of all channels (h_sens null) or taken from h_sens (num_voxels).
- * The matrix is built once and kept resident for all iterations. */
+ * The matrix and its transpose are built once and kept resident for all
+ * iterations; when they do not fit the device (an allocation fails), the
+ * call goes on as raptr_mlem_stream with the rows that fit kept resident
+ * and the others rebuilt in every iteration (stats->streamed_rows). */
 raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_y, int32_t nrays, uint32_t seed,
                              int32_t n_iter, const float* h_sens, const float* h_x0, float* h_x,
                              raptr_reco_stats* stats);

@@ -72,6 +72,11 @@ class raptr_server_stats(C.Structure):
                                          "resident_matrices", "resident_bytes", "queued", "running")]
 
 
+class raptr_stream_stats(C.Structure):
+    _fields_ = [("resident_rows", C.c_int64), ("resident_entries", C.c_int64), ("streamed_rows", C.c_int64),
+                ("level", C.c_int32), ("first_iter_ms", C.c_double), ("iter_ms", C.c_double)]
+
+
 class raptr_reco_stats(C.Structure):
     _fields_ = [
         ("build_ms", C.c_double),
@@ -81,6 +86,13 @@ class raptr_reco_stats(C.Structure):
         ("nnz", C.c_int64),
         ("h2d_bytes", C.c_int64),
         ("d2h_bytes", C.c_int64),
+        ("transpose_ms", C.c_double),
+        ("inputs_ms", C.c_double),
+        ("output_ms", C.c_double),
+        ("setup_ms", C.c_double),
+        ("release_ms", C.c_double),
+        ("wall_ms", C.c_double),
+        ("streamed_rows", C.c_int64),
     ]
 
 
@@ -149,6 +161,8 @@ _SIGNATURES = {
     "raptr_csr_transpose": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_csr_transpose_ordered": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_mlem_noalloc": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, I32, VP]),
+    "raptr_mlem_stream": (C.c_int, [VP, VP, I64, I32, C.c_uint32, VP, VP, VP, VP, I32, I64,
+                                    C.POINTER(raptr_stream_stats), VP]),
     "raptr_row_ptr_narrow": (C.c_int, [VP, I64, VP, VP]),
     "raptr_row_ptr_widen": (C.c_int, [VP, I64, VP, VP]),
     "raptr_reco_host": (C.c_int, [C.POINTER(raptr_geom), C.c_int, VP, I32, C.c_uint32, I32, VP, VP, VP,
@@ -419,6 +433,20 @@ class Context:
             out.append(np.array(kt[:2 * niter], np.float64).reshape(niter, 2))
         return None if not out else (out[0] if len(out) == 1 else tuple(out))
 
+
+    def mlem_stream(self, cnl, nrays: int, seed: int, y, s, x, niter: int, resident_bytes: int, s_out=None,
+                    stream=None) -> dict:
+        """MLEM over the rows of the listed channels without storing the
+        whole matrix: the leading rows that fit resident_bytes are kept after
+        the first iteration, the others are rebuilt in every iteration
+        (raptr_mlem_stream).  y: counts of the listed channels; s: the
+        normalised sensitivity or None (computed; written to s_out when
+        given); x updated in place.  Returns the call's statistics."""
+        lst = self._list(cnl)
+        st = raptr_stream_stats()
+        _check(lib().raptr_mlem_stream(self._h, _ptr(lst), lst.numel(), nrays, seed, _ptr(y), _ptr(s), _ptr(s_out),
+                                       _ptr(x), niter, int(resident_bytes), C.byref(st), _stream(stream)))
+        return {k: getattr(st, k) for k, _ in raptr_stream_stats._fields_}
 
     def mlem_half(self, A: Matrix, y, s, x, niter: int, use_graph: bool = True, loglik: bool = False,
                   kernel_times: bool = False, stream=None):

@@ -1423,11 +1423,7 @@ raptr_status batch_args(raptr_ctx* ctx, int64_t m, int64_t n, int32_t K, int32_t
   return RAPTR_OK;
 }
 
-int default_frame_tile(int K) {
-  for (int kt : {32, 16, 8, 4, 64})
-    if (batch_tile_supported(K, kt)) return kt;
-  return 0;
-}
+int default_frame_tile(int K) { return batch_tile_supported(K, 32) ? 32 : 0; }
 
 }  // namespace
 
@@ -1443,7 +1439,7 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
   if (n_iter < 0) return fail(RAPTR_ERR_INVALID, "bad argument");
   const int kt = frame_tile > 0 ? frame_tile : default_frame_tile(n_frames);
   if (!batch_tile_supported(n_frames, kt))
-    return fail(RAPTR_ERR_INVALID, "frame tile must be 4, 8, 16, 32 or 64 and divide the number of frames");
+    return fail(RAPTR_ERR_INVALID, "the number of frames must be a multiple of 4 and the frame tile 4, 8, 16, 32 or 64");
   if (n_iter == 0) return RAPTR_OK;
   DeviceScope ds(ctx->device);
   cudaStream_t s = as_stream(stream);
@@ -1567,6 +1563,160 @@ raptr_status raptr_mlem_batch_autotune(raptr_ctx* ctx, int64_t m, int64_t n, int
   return RAPTR_OK;
 }
 
+raptr_status raptr_mlem_stream(raptr_ctx* ctx, const int32_t* d_cnl, int64_t n_list, int32_t nrays, uint32_t seed,
+                               const float* d_y, const float* d_s, float* d_s_out, float* d_x, int32_t n_iter,
+                               int64_t resident_bytes, raptr_stream_stats* stats, void* stream) {
+  if (!ctx || n_list < 0 || (n_list > 0 && (!d_cnl || !d_y)) || nrays <= 0 || n_iter < 0 || !d_x ||
+      resident_bytes < 0)
+    return fail(RAPTR_ERR_INVALID, "bad argument");
+  if (stats) *stats = raptr_stream_stats{};
+  if (n_iter == 0) return RAPTR_OK;
+  DeviceScope ds(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  const int64_t N = raptr_ctx_num_voxels(ctx);
+  // resident CSR of the leading rows: row pointers for every row, entries
+  // up to what resident_bytes leaves after them
+  const int64_t rp_bytes = (n_list + 1) * int64_t(sizeof(int64_t));
+  const int64_t cap = resident_bytes > rp_bytes ? (resident_bytes - rp_bytes) / 8 : 0;
+  int64_t* rp = nullptr;
+  int32_t* rcol = nullptr;
+  float* rval = nullptr;
+  float *c = nullptr, *s32 = nullptr;
+  double* s64 = nullptr;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  struct Owned {
+    std::function<void()> f;
+    ~Owned() { f(); }
+  } owned{[&] {
+    dev_free(rp);
+    dev_free(rcol);
+    dev_free(rval);
+    dev_free(c);
+    dev_free(s32);
+    dev_free(s64);
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }};
+  for (auto& e : ev) RCU(cudaEventCreate(&e));
+  if (cap > 0) {
+    RCU(dev_malloc(&rp, size_t(rp_bytes)));
+    RCU(dev_malloc(&rcol, size_t(cap) * sizeof(int32_t)));
+    RCU(dev_malloc(&rval, size_t(cap) * sizeof(float)));
+  }
+  RCU(dev_malloc(&c, size_t(N) * sizeof(float)));
+  if (!d_s) {
+    RCU(dev_malloc(&s64, size_t(N) * sizeof(double)));
+    RCU(dev_malloc(&s32, size_t(N) * sizeof(float)));
+  }
+  const float* s_use = d_s ? d_s : s32;
+  double* acc = ctx->d_f64;  // [0]: image sum, [1]: sensitivity sum
+  int level = sm_pick_level(ctx->dg, nrays);
+  int64_t n_res = 0, n_ent = 0;
+  volatile int64_t* h_words = nullptr;
+  if (!ctx->h_pin) RCU(cudaMallocHost(&ctx->h_pin, 16 * sizeof(int64_t)));
+  h_words = ctx->h_pin;
+  volatile int32_t* h_flags = reinterpret_cast<volatile int32_t*>(const_cast<int64_t*>(h_words + 4));
+
+  // Builds rows [from, n_list) chunk by chunk and projects them from the
+  // staging; in the first iteration also keeps the leading chunks that fit
+  // the resident CSR.
+  auto sweep = [&](bool first, int64_t from) -> raptr_status {
+    const int H = sm_level_capacity(level);
+    int64_t per = std::max<int64_t>(1, int64_t(kStagingBudget / (size_t(H) * 8)));
+    per = std::min<int64_t>(per, 65536);
+    RCHECK(ctx->ensure_scratch(Carve::need({size_t(per) * H * sizeof(int32_t), size_t(per) * H * sizeof(float),
+                                            size_t(per) * sizeof(int32_t)})));
+    Carve cv(ctx->d_scratch);
+    int32_t* st_col = cv.take<int32_t>(size_t(per) * H);
+    float* st_val = cv.take<float>(size_t(per) * H);
+    int32_t* row_nnz = cv.take<int32_t>(size_t(per));
+    bool open = first && cap > 0;
+    for (int64_t r = from; r < n_list; r += per) {
+      const int64_t k = std::min(per, n_list - r);
+      RCU(launch_sm_rows(level, ctx->dg, ctx->d_sincos, d_cnl, r, k, nrays, seed, nullptr, st_col, st_val, row_nnz,
+                         ctx->d_flags, s));
+      RCU(launch_stage_project(k, st_col, st_val, H, row_nnz, d_y + r, d_x, c, first ? s64 : nullptr, s));
+      if (!open) continue;
+      RCU(launch_rows_scan(row_nnz, k, rp + r, ctx->d_i64, s));
+      RCU(cudaMemcpyAsync(const_cast<int64_t*>(h_words), ctx->d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      RCU(cudaMemcpyAsync(const_cast<int32_t*>(h_flags), ctx->d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      RCU(cudaStreamSynchronize(s));
+      const int64_t total = h_words[0];
+      if (*h_flags != 0) {
+        open = false;  // redone a level up anyway
+        continue;
+      }
+      int64_t keep = k, kept_entries = total;
+      if (total > cap) {
+        // the chunk's leading rows that still fit; the rest of it and every
+        // later chunk are rebuilt in every iteration
+        std::vector<int64_t> h_rp(size_t(k) + 1);
+        RCU(cudaMemcpy(h_rp.data(), rp + r, h_rp.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        keep = int64_t(std::upper_bound(h_rp.begin(), h_rp.end(), cap) - h_rp.begin()) - 1;
+        kept_entries = h_rp[size_t(keep)];
+        open = false;
+      }
+      if (keep > 0) RCU(launch_rows_gather(st_col, st_val, H, rp + r, keep, cap, rcol, rval, s));
+      n_res = r + keep;
+      n_ent = kept_entries;
+    }
+    return RAPTR_OK;
+  };
+
+  for (int32_t it = 0; it < n_iter; it++) {
+    const bool first = it == 0;
+    if (first) RCU(cudaEventRecord(ev[0], s));
+    RCU(cudaMemsetAsync(ctx->d_flags, 0, sizeof(int32_t), s));
+    if (first) {
+      n_res = n_ent = 0;
+      RCU(cudaMemsetAsync(c, 0, size_t(N) * sizeof(float), s));
+      RCU(cudaMemsetAsync(ctx->d_i64, 0, sizeof(int64_t), s));
+      if (s64) RCU(cudaMemsetAsync(s64, 0, size_t(N) * sizeof(double), s));
+    } else if (n_res > 0) {
+      RCU(launch_mlem_project(n_res, rp, rcol, rval, d_y, d_x, c, nullptr, s));
+    }
+    RCHECK(sweep(first, first ? 0 : n_res));
+    RCU(cudaMemcpyAsync(const_cast<int32_t*>(h_flags), ctx->d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    RCU(cudaStreamSynchronize(s));
+    const int32_t flags = *h_flags;
+    if (flags & 4) return fail(RAPTR_ERR_INVALID, "a channel id is outside [0, number of channels)");
+    if (flags & 2) return fail(RAPTR_ERR_OVERFLOW, "ray walk did not terminate (internal error)");
+    if (flags & 1) {
+      // a row has more distinct voxels than the level's table: redo the
+      // first iteration (nothing of it has been applied) a level up
+      if (!first || level + 1 >= sm_num_levels())
+        return fail(RAPTR_ERR_OVERFLOW, "a row has more distinct voxels than the largest per-row table holds");
+      level++;
+      it = -1;
+      continue;
+    }
+    if (first && s64) {
+      RCU(cudaMemsetAsync(acc + 1, 0, sizeof(double), s));
+      RCU(launch_sum_f64(s64, N, acc + 1, s));
+      RCU(launch_sens_normalise(N, s64, acc + 1, s32, s));
+    }
+    if (first && d_s_out) RCU(cudaMemcpyAsync(d_s_out, s_use, size_t(N) * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    RCU(cudaMemsetAsync(acc, 0, sizeof(double), s));
+    RCU(launch_mlem_update(N, d_x, c, s_use, acc, s));
+    RCU(launch_mlem_normalise(N, d_x, c, acc, s));  // also clears c for the next iteration
+    if (first) RCU(cudaEventRecord(ev[1], s));
+  }
+  RCU(cudaEventRecord(ev[2], s));
+  RCU(cudaStreamSynchronize(s));
+  if (stats) {
+    float t01 = 0.f, t12 = 0.f;
+    cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    cudaEventElapsedTime(&t12, ev[1], ev[2]);
+    stats->resident_rows = n_res;
+    stats->resident_entries = n_ent;
+    stats->streamed_rows = n_list - n_res;
+    stats->level = level;
+    stats->first_iter_ms = t01;
+    stats->iter_ms = n_iter > 1 ? t12 / double(n_iter - 1) : 0.0;
+  }
+  return RAPTR_OK;
+}
+
 raptr_status raptr_mlem_noalloc(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
                                 const float* d_val, const float* d_y, const float* d_s, float* d_x, int32_t n_iter,
                                 void* stream) {
@@ -1582,6 +1732,7 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
                              int32_t n_iter, const float* h_sens, const float* h_x0, float* h_x,
                              raptr_reco_stats* stats) {
   if (!h_y || !h_x || nrays <= 0 || n_iter < 0) return fail(RAPTR_ERR_INVALID, "bad argument");
+  const double t_call = trace_ms();
   trace("reco_host: start");
   raptr_ctx* ctx = nullptr;
   RCHECK(raptr_ctx_create(geom, device, &ctx));
@@ -1589,8 +1740,12 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
   const int64_t M = raptr_ctx_num_channels(ctx), N = raptr_ctx_num_voxels(ctx);
   cudaStream_t s;
   RCU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  cudaEvent_t ev[5];
+  // events: 0 start, 1 inputs on the device, 2 matrix built, 3 transpose
+  // built, 4 sensitivity and start image ready, 5 iterations done, 6 image
+  // on the host
+  cudaEvent_t ev[7];
   for (auto& e : ev) cudaEventCreate(&e);
+  const double t_setup = trace_ms();
   raptr_matrix* A = nullptr;
   float *d_y = nullptr, *d_x = nullptr, *d_s = nullptr;
   int32_t* d_list = nullptr;
@@ -1616,6 +1771,14 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
       return st;                                            \
     }                                                       \
   } while (0)
+#define RSTATUS()                                           \
+  do {                                                      \
+    if (st != RAPTR_OK) {                                   \
+      std::string msg = g_last_error;                       \
+      cleanup();                                            \
+      return fail(st, msg);                                 \
+    }                                                       \
+  } while (0)
   RSTEP(cudaEventRecord(ev[0], s));
   RSTEP(dev_malloc(&d_y, size_t(M) * sizeof(float)));
   RSTEP(dev_malloc(&d_x, size_t(N) * sizeof(float)));
@@ -1628,22 +1791,27 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
   trace("reco_host: inputs on the device");
   st = raptr_sm_build_alloc(ctx, d_list, M, nrays, seed, nullptr, 0, &A, s);
   trace("reco_host: matrix built");
-  if (st != RAPTR_OK) {
-    std::string msg = g_last_error;
-    cleanup();
-    return fail(st, msg);
-  }
-  st = raptr_matrix_transpose(A, s);
-  trace("reco_host: transpose built");
-  if (st != RAPTR_OK) {
-    std::string msg = g_last_error;
-    cleanup();
-    return fail(st, msg);
-  }
   RSTEP(cudaEventRecord(ev[2], s));
+  if (st == RAPTR_OK) st = raptr_matrix_transpose(A, s);
+  trace("reco_host: transpose built");
+  RSTEP(cudaEventRecord(ev[3], s));
+  // A matrix and transpose that do not fit the device: rebuild rows in every
+  // iteration instead (raptr_mlem_stream), keeping as many as fit.
+  const bool streamed = st == RAPTR_ERR_NOMEM;
+  if (streamed) {
+    raptr_matrix_destroy(A);
+    A = nullptr;
+    dev_release(device);
+    trace("reco_host: the matrix does not fit: rows are rebuilt in every iteration");
+  } else {
+    RSTATUS();
+  }
   if (!h_sens) {
-    RSTEP(dev_malloc(&d_s64, size_t(N) * sizeof(double)));
-    st = raptr_sensitivity(A->m, N, A->rp, A->col, A->val, d_s64, d_s, s);
+    if (!streamed) {
+      RSTEP(dev_malloc(&d_s64, size_t(N) * sizeof(double)));
+      st = raptr_sensitivity(A->m, N, A->rp, A->col, A->val, d_s64, d_s, s);
+      RSTATUS();
+    }
   } else {
     RSTEP(cudaMemcpyAsync(d_s, h_sens, size_t(N) * sizeof(float), cudaMemcpyHostToDevice, s));
     h2d += N * int64_t(sizeof(float));
@@ -1653,11 +1821,6 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
     RSTEP(cudaMemcpyAsync(&sum, ctx->d_f64, sizeof(double), cudaMemcpyDeviceToHost, s));
     RSTEP(cudaStreamSynchronize(s));
     RSTEP(launch_scales(d_s, float(1. / float(sum)), N, s));
-  }
-  if (st != RAPTR_OK) {
-    std::string msg = g_last_error;
-    cleanup();
-    return fail(st, msg);
   }
   if (h_x0) {
     RSTEP(cudaMemcpyAsync(d_x, h_x0, size_t(N) * sizeof(float), cudaMemcpyHostToDevice, s));
@@ -1669,37 +1832,52 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
     RSTEP(cudaStreamSynchronize(s));
     h2d += N * int64_t(sizeof(float));
   }
-  RSTEP(cudaEventRecord(ev[3], s));
-  raptr_mlem_opts o{1, nullptr, nullptr, A->rank};
-  trace("reco_host: sensitivity");
-  st = raptr_mlem(ctx, A->m, N, A->rp, A->col, A->val, A->cp, A->trow, A->tval, d_y, d_s, d_x, n_iter, &o, s);
-  trace("reco_host: iterations enqueued");
-  if (st != RAPTR_OK) {
-    std::string msg = g_last_error;
-    cleanup();
-    return fail(st, msg);
-  }
   RSTEP(cudaEventRecord(ev[4], s));
-  RSTEP(cudaMemcpyAsync(h_x, d_x, size_t(N) * sizeof(float), cudaMemcpyDeviceToHost, s));
-  RSTEP(cudaStreamSynchronize(s));
-  if (stats) {
-    float t;
-    cudaEventElapsedTime(&t, ev[1], ev[2]);
-    stats->build_ms = t;
-    cudaEventElapsedTime(&t, ev[2], ev[3]);
-    stats->sens_ms = t;
-    cudaEventElapsedTime(&t, ev[3], ev[4]);
-    stats->iter_ms = t;
-    cudaEventElapsedTime(&t, ev[0], ev[4]);
-    stats->total_ms = t;
-    stats->nnz = A->nnz;
-    stats->h2d_bytes = h2d;
-    stats->d2h_bytes = N * int64_t(sizeof(float));
+  trace("reco_host: sensitivity");
+  raptr_stream_stats sst{};
+  if (streamed) {
+    // what the device holds now, less the row staging and working vectors
+    size_t free_b = 0, total_b = 0;
+    RSTEP(cudaMemGetInfo(&free_b, &total_b));
+    const int64_t reserve = (int64_t(3) << 30) + N * 24;
+    const int64_t resident = std::max<int64_t>(0, (int64_t(free_b) - reserve) * 9 / 10);
+    st = raptr_mlem_stream(ctx, d_list, M, nrays, seed, d_y, h_sens ? d_s : nullptr, nullptr, d_x, n_iter, resident,
+                           &sst, s);
+  } else {
+    raptr_mlem_opts o{1, nullptr, nullptr, A->rank};
+    st = raptr_mlem(ctx, A->m, N, A->rp, A->col, A->val, A->cp, A->trow, A->tval, d_y, d_s, d_x, n_iter, &o, s);
   }
+  trace("reco_host: iterations enqueued");
+  RSTATUS();
+  RSTEP(cudaEventRecord(ev[5], s));
+  RSTEP(cudaMemcpyAsync(h_x, d_x, size_t(N) * sizeof(float), cudaMemcpyDeviceToHost, s));
+  RSTEP(cudaEventRecord(ev[6], s));
+  RSTEP(cudaStreamSynchronize(s));
+  const double t_image = trace_ms();
+  const int64_t nnz = A ? A->nnz : sst.resident_entries;
+  float t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int i = 0; i < 6; i++) cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
 #undef RSTEP
+#undef RSTATUS
   trace("reco_host: image on the host");
   cleanup();
   trace("reco_host: device memory released");
+  if (stats) {
+    stats->build_ms = t[1];
+    stats->sens_ms = t[3];
+    stats->iter_ms = t[4];
+    stats->total_ms = t[0] + t[1] + t[2] + t[3] + t[4] + t[5];
+    stats->nnz = nnz;
+    stats->h2d_bytes = h2d;
+    stats->d2h_bytes = N * int64_t(sizeof(float));
+    stats->transpose_ms = t[2];
+    stats->inputs_ms = t[0];
+    stats->output_ms = t[5];
+    stats->setup_ms = t_setup - t_call;
+    stats->release_ms = trace_ms() - t_image;
+    stats->wall_ms = trace_ms() - t_call;
+    stats->streamed_rows = streamed ? sst.streamed_rows : 0;
+  }
   return RAPTR_OK;
 }
 

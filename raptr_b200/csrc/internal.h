@@ -119,6 +119,13 @@ cudaError_t launch_sum_f64(const double* x, int64_t n, double* d_acc, cudaStream
 cudaError_t launch_mlem_project(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const float* y,
                                 const float* x, float* c, double* d_ll, cudaStream_t s);
 // x = x*c/(s + (s==0)); d_acc[0] += sum(x) (FP64).
+// The projection of launch_mlem_project for rows in the build's staging
+// slots (row i at st_col/st_val + i*cap, row_nnz[i] entries; rows with
+// row_nnz < 0 skipped); with s64 non-null also s64[col] += val (FP64) for
+// every built row.
+cudaError_t launch_stage_project(int64_t nrows, const int32_t* st_col, const float* st_val, int cap,
+                                 const int32_t* row_nnz, const float* y, const float* x, float* c, double* s64,
+                                 cudaStream_t s);
 cudaError_t launch_mlem_update(int64_t n, float* x, const float* c, const float* sens, double* d_acc, cudaStream_t s);
 // x *= float(1/float(d_acc[0])); c = 0; d_acc[0] reset by the next project.
 cudaError_t launch_mlem_normalise(int64_t n, float* x, float* c, double* d_acc, cudaStream_t s);
@@ -176,10 +183,14 @@ struct BatchArgs {
   float* E = nullptr;
   float* XX = nullptr;
 };
+// K frames (a multiple of 4) in tiles of at most kt (4, 8, 16, 32 or 64).
 bool batch_tile_supported(int K, int kt);
-// One iteration for all K frames in tiles of kt frames (acc: K doubles,
-// next: K/kt work counters, both scratch); ev_mid, when set, is recorded
-// between the two passes.
+// The tile that starts at frame f0: kt while kt frames remain, else the
+// largest power of two that fits.
+int batch_tile_at(int K, int kt, int f0);
+// One iteration for all K frames in tiles of at most kt frames (acc: K
+// doubles, next: K/4 work counters, both scratch); ev_mid, when set, is
+// recorded between the two passes.
 cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, unsigned long long* next, cudaStream_t s,
                                    cudaEvent_t ev_mid);
 

@@ -233,25 +233,37 @@ cudaError_t launch_tile_kt(int kt, bool forward, int64_t m, int64_t n, int K, in
 }  // namespace
 
 bool batch_tile_supported(int K, int kt) {
-  return (kt == 4 || kt == 8 || kt == 16 || kt == 32 || kt == 64) && K > 0 && K % kt == 0;
+  return (kt == 4 || kt == 8 || kt == 16 || kt == 32 || kt == 64) && K > 0 && K % 4 == 0;
+}
+
+int batch_tile_at(int K, int kt, int f0) {
+  int t = kt;
+  while (t > K - f0) t >>= 1;
+  return t;
 }
 
 cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, unsigned long long* next, cudaStream_t s,
                                    cudaEvent_t ev_mid) {
+  // Tiles of kt frames while that many remain, then the largest power of
+  // two (>= 4, since K is a multiple of 4) that fits: 40 frames at kt = 32
+  // run as 32 + 8, so no frame slot is computed for nothing.
   cudaError_t e = cudaMemsetAsync(acc, 0, size_t(a.K) * sizeof(double), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(next, 0, size_t(a.K / kt) * sizeof(unsigned long long), s);
-  for (int f0 = 0; f0 < a.K && e == cudaSuccess; f0 += kt)
-    e = a.half ? launch_tile_kt<__half>(kt, true, a.m, a.n, a.K, f0, a.rp, a.col, a.val, a.rscale, a.cp, a.trow,
+  if (e == cudaSuccess) e = cudaMemsetAsync(next, 0, size_t(a.K / 4) * sizeof(unsigned long long), s);
+  for (int f0 = 0; f0 < a.K && e == cudaSuccess; f0 += batch_tile_at(a.K, kt, f0)) {
+    const int t = batch_tile_at(a.K, kt, f0);
+    e = a.half ? launch_tile_kt<__half>(t, true, a.m, a.n, a.K, f0, a.rp, a.col, a.val, a.rscale, a.cp, a.trow,
                                         a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, nullptr, s)
-               : launch_tile_kt<float>(kt, true, a.m, a.n, a.K, f0, a.rp, a.col, a.val, nullptr, a.cp, a.trow,
+               : launch_tile_kt<float>(t, true, a.m, a.n, a.K, f0, a.rp, a.col, a.val, nullptr, a.cp, a.trow,
                                        a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, nullptr, s);
+  }
   if (e == cudaSuccess && ev_mid) e = cudaEventRecord(ev_mid, s);
-  for (int f0 = 0; f0 < a.K && e == cudaSuccess; f0 += kt)
-    e = a.half ? launch_tile_kt<__half>(kt, false, a.m, a.n, a.K, f0, a.rp, a.col, a.val, a.rscale, a.cp, a.trow,
-                                        a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, next + f0 / kt,
-                                        s)
-               : launch_tile_kt<float>(kt, false, a.m, a.n, a.K, f0, a.rp, a.col, a.val, nullptr, a.cp, a.trow,
-                                       a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, next + f0 / kt, s);
+  for (int f0 = 0, tile = 0; f0 < a.K && e == cudaSuccess; f0 += batch_tile_at(a.K, kt, f0), tile++) {
+    const int t = batch_tile_at(a.K, kt, f0);
+    e = a.half ? launch_tile_kt<__half>(t, false, a.m, a.n, a.K, f0, a.rp, a.col, a.val, a.rscale, a.cp, a.trow,
+                                        a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, next + tile, s)
+               : launch_tile_kt<float>(t, false, a.m, a.n, a.K, f0, a.rp, a.col, a.val, nullptr, a.cp, a.trow,
+                                       a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, next + tile, s);
+  }
   if (e == cudaSuccess) {
     const int64_t total = a.n * a.K;
     int64_t blocks = (total + kThreads - 1) / kThreads;

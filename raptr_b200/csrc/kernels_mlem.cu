@@ -280,6 +280,36 @@ __global__ void __launch_bounds__(kThreads) mlem_project_kernel(int64_t m, const
   }
 }
 
+// The same projection for rows still in the build's staging slots (row i:
+// entries st_col/st_val[i*cap, i*cap + row_nnz[i]), columns ascending), so
+// that rows rebuilt in every iteration are projected without being placed
+// into a CSR first.  Rows with row_nnz[i] < 0 (not built) are skipped.
+// With s64 non-null every built row's entries are also added to the FP64
+// column sums s64 (the sensitivity), measured or not.
+__global__ void __launch_bounds__(kThreads) stage_project_kernel(int64_t nrows, const int32_t* __restrict__ st_col,
+                                                                 const float* __restrict__ st_val, int cap,
+                                                                 const int32_t* __restrict__ row_nnz,
+                                                                 const float* __restrict__ y,
+                                                                 const float* __restrict__ x, float* __restrict__ c,
+                                                                 double* __restrict__ s64) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < nrows; r += nw) {
+    const int cnt = __ldg(row_nnz + r);
+    if (cnt <= 0) continue;
+    const int32_t* rc = st_col + size_t(r) * cap;
+    const float* rv = st_val + size_t(r) * cap;
+    if (s64)
+      for (int k = lane; k < cnt; k += 32) atomicAdd(s64 + __ldg(rc + k), double(__ldg(rv + k)));
+    const float yi = __ldg(y + r);
+    if (yi == 0.f) continue;
+    float acc = 0.f;
+    for (int k = lane; k < cnt; k += 32) acc += __ldg(rv + k) * __ldg(x + __ldg(rc + k));
+    const float f = __fdiv_rn(yi, warp_sum(acc));
+    for (int k = lane; k < cnt; k += 32) atomicAdd(c + __ldg(rc + k), __ldg(rv + k) * f);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) mlem_update_kernel(int64_t n, float* __restrict__ x,
                                                                const float* __restrict__ c,
                                                                const float* __restrict__ s, double* __restrict__ acc) {
@@ -610,6 +640,16 @@ cudaError_t launch_mlem_project(int64_t m, const int64_t* rp, const int32_t* col
       mlem_project_kernel<false><<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, y, x, c, d_ll);
       note_launches(1);
     }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage_project(int64_t nrows, const int32_t* st_col, const float* st_val, int cap,
+                                 const int32_t* row_nnz, const float* y, const float* x, float* c, double* s64,
+                                 cudaStream_t s) {
+  if (nrows > 0) {
+    stage_project_kernel<<<row_grid(nrows), kThreads, 0, s>>>(nrows, st_col, st_val, cap, row_nnz, y, x, c, s64);
+    note_launches(1);
   }
   return cudaGetLastError();
 }

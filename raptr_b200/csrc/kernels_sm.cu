@@ -26,6 +26,7 @@
 //
 // This translation unit is compiled with -fmad=false in addition to the
 // explicit round-to-nearest intrinsics used on every exact path.
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 
@@ -60,6 +61,13 @@ __device__ __forceinline__ float plane_alpha_r(float o, float d, int i, float r0
   if (!(fabsf(dir) >= 1e-30f && fabsf(dir) <= 1e30f)) return RFDIV(num, dir);
   return div_rcp(num, dir, rc);
 }
+
+// Origin, pitch and size of axis k of the grid for a k known only at run
+// time: selects, so that the by-value geometry stays in the constant bank
+// instead of being copied to local memory for an indexed access.
+__device__ __forceinline__ float axis_o(const DGeom& g, int k) { return k == 0 ? g.o[0] : (k == 1 ? g.o[1] : g.o[2]); }
+__device__ __forceinline__ float axis_d(const DGeom& g, int k) { return k == 0 ? g.d[0] : (k == 1 ? g.d[1] : g.d[2]); }
+__device__ __forceinline__ int axis_n(const DGeom& g, int k) { return k == 0 ? g.n[0] : (k == 1 ? g.n[1] : g.n[2]); }
 
 // Shared-memory accumulation table: keys (voxel id, -1 = empty) and sums.
 template <int H>
@@ -511,34 +519,83 @@ __device__ inline void slab_window(const DGeom& g, int a, const float plo[3], co
       whi = fmaxf(whi, phi[w] + t * (qhi[w] - phi[w]));
     }
   }
-  const int n = g.n[w];
-  int lo = int(floorf((wlo - g.o[w]) / g.d[w])) - 1;
-  int hi = int(floorf((whi - g.o[w]) / g.d[w])) + 1;
+  const int n = axis_n(g, w);
+  int lo = int(floorf((wlo - axis_o(g, w)) / axis_d(g, w))) - 1;
+  int hi = int(floorf((whi - axis_o(g, w)) / axis_d(g, w))) + 1;
   lo = min(max(lo, 0), n - 1);
   hi = min(max(hi, 0), n - 1);
   *ilo = lo;
   *ihi = max(lo, hi);
 }
 
-// One CTA per row (channel): its rays are walked by the CTA's threads and
-// their lengths summed per voxel in shared memory, then the voxels that pass
-// the cylinder test are written in column order to the row's staging slot.
-// The sums go to dense slab windows when the row allows it (generated rays,
-// crystals on opposite sides of the grid along x or z, windows within
-// dense_slots(H) slots), else to an open-addressing hash table of H keys; a dense row that
-// finds a voxel outside its windows is redone with the table.
+// Row status the dense kernel leaves for the table kernel: the row is to be
+// built with the hash table (it does not qualify for dense windows, or a
+// ray left its windows).
+constexpr int kRowToTable = -2;
+
+// Bitonic sort of (keys, vals)[0, total) by key in shared memory (npad =
+// the next power of two, padded with INT_MAX), then written to the row's
+// staging slot and its length to *row_nnz.  Every thread of the CTA calls it.
+template <int T>
+__device__ void sort_and_write(int* keys, float* vals, int total, int32_t* __restrict__ st_col,
+                               float* __restrict__ st_val, size_t base, int32_t* row_nnz) {
+  const int tid = threadIdx.x;
+  int npad = 1;
+  while (npad < total) npad <<= 1;
+  for (int i = total + tid; i < npad; i += T) keys[i] = INT_MAX;
+  __syncthreads();
+  for (int k = 2; k <= npad; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = tid; t < (npad >> 1); t += T) {
+        int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+        int p = i | j;
+        bool asc = (i & k) == 0;
+        int ki = keys[i], kp = keys[p];
+        if ((ki > kp) == asc) {
+          keys[i] = kp;
+          keys[p] = ki;
+          float vi = vals[i];
+          vals[i] = vals[p];
+          vals[p] = vi;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = tid; i < total; i += T) {
+    st_col[base + i] = keys[i];
+    st_val[base + i] = vals[i];
+  }
+  if (tid == 0) *row_nnz = total;
+}
+
+// Dense kernel: one CTA per row whose two crystals lie on opposite sides of
+// the grid along x or z (generated rays only).  Every ray of such a row
+// crosses the grid in the same direction along that slab axis and lies in
+// the convex hull of the two crystal boxes, so the voxels its rays reach lie
+// in per-slab windows, and the lengths are summed into dense slots of those
+// windows: no key is stored, loaded or compared.  The voxels with a positive
+// sum that pass the cylinder test are written in column order (x slabs are
+// in column order already; z slabs are sorted).  A row that does not
+// qualify, whose windows exceed dense_slots(H), or one of whose rays leaves
+// its windows gets row_nnz = kRowToTable and is built by sm_table_kernel.
+// Why the windows hold every voxel a ray visits: the hull bound is exact in
+// real arithmetic, the walk visits voxels adjacent to the real ray's voxels
+// at worst (rounding at plane ties), and the windows have a margin of one
+// voxel on each side; the spare slot and the compaction's decode check
+// catch a slot outside the windows' range regardless.
 template <int H, int T, bool OISO>
-__global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __restrict__ sincos,
-                                                    const int32_t* __restrict__ cnl_ids, int64_t row0, int nrays,
-                                                    uint32_t seed, const float* __restrict__ rays,
-                                                    int32_t* __restrict__ st_col, float* __restrict__ st_val,
-                                                    int32_t* __restrict__ row_nnz, int32_t* __restrict__ flags) {
+__global__ void __launch_bounds__(T) sm_dense_kernel(DGeom g, const float2* __restrict__ sincos,
+                                                     const int32_t* __restrict__ cnl_ids, int64_t row0, int nrays,
+                                                     uint32_t seed, int32_t* __restrict__ st_col,
+                                                     float* __restrict__ st_val, int32_t* __restrict__ row_nnz,
+                                                     int32_t* __restrict__ flags) {
   extern __shared__ __align__(16) unsigned char smem[];
-  int* keys = reinterpret_cast<int*>(smem);
+  float* acc = reinterpret_cast<float*>(smem);  // dense_slots(H) slots + the spare one
+  int* keys = reinterpret_cast<int*>(smem);     // z slabs: the row's entries for the sort
   float* vals = reinterpret_cast<float*>(smem + H * sizeof(int));
-  float* acc = reinterpret_cast<float*>(smem);  // dense mode: dense_slots(H) slots over the same memory
   __shared__ Channel ch;
-  __shared__ int overflow, bad_walk, dense_fail, win_u, win_v, sax, sdir;
+  __shared__ int bad_walk, dense_fail, win_u, win_v, sax, sdir;
   __shared__ float box_lo[2][3], box_hi[2][3];
   __shared__ int warp_sums[32];
   __shared__ int ulo[kMaxSlabs], vlo[kMaxSlabs], sbase[kMaxSlabs], sdk[kMaxSlabs];
@@ -553,45 +610,44 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     }
     return;
   }
-
   const int nyz = g.n[1] * g.n[2];
   const int nz = g.n[2];
   if (tid == 0) {
     channel_setup(g, sincos, cnl, ch);
-    overflow = 0;
     bad_walk = 0;
     dense_fail = 0;
     win_u = 0;
     win_v = 0;
+    crystal_boxes(ch, box_lo, box_hi);
+    // the slab axis: of x and z, the one along which the crystals lie on
+    // opposite sides of the grid, the channel's dominant direction first
+    // (its windows are the narrowest)
     int axis = -1, dir = 0;
-    if (!rays) {
-      crystal_boxes(ch, box_lo, box_hi);
-      // the slab axis: of x and z, the one along which the crystals lie
-      // on opposite sides of the grid, the channel's dominant direction
-      // first (its windows are the narrowest)
-      const int first = fabsf(ch.ab[0]) >= fabsf(ch.ab[2]) ? 0 : 2;
-      for (int k = 0; k < 2 && axis < 0; k++) {
-        const int a = k == 0 ? first : 2 - first;
-        if (g.n[a] > kMaxSlabs) continue;
-        const float c0 = g.o[a], c1 = g.o[a] + float(g.n[a]) * g.d[a];
-        const float m = 1e-6f * (1.0f + fabsf(c0) + fabsf(c1));
-        if (box_hi[0][a] + m < c0 && box_lo[1][a] - m > c1) dir = 1;
-        if (box_hi[1][a] + m < c0 && box_lo[0][a] - m > c1) dir = -1;
-        if (dir != 0) axis = a;
-      }
+    const int first = fabsf(ch.ab[0]) >= fabsf(ch.ab[2]) ? 0 : 2;
+    for (int k = 0; k < 2 && axis < 0; k++) {
+      const int a = k == 0 ? first : 2 - first;
+      if (axis_n(g, a) > kMaxSlabs) continue;
+      const float c0 = axis_o(g, a), c1 = axis_o(g, a) + float(axis_n(g, a)) * axis_d(g, a);
+      const float m = 1e-6f * (1.0f + fabsf(c0) + fabsf(c1));
+      if (box_hi[0][a] + m < c0 && box_lo[1][a] - m > c1) dir = 1;
+      if (box_hi[1][a] + m < c0 && box_lo[0][a] - m > c1) dir = -1;
+      if (dir != 0) axis = a;
     }
     sax = axis;
     sdir = dir;
   }
   __syncthreads();
-
   const int A = sax;
+  if (A < 0) {
+    if (tid == 0) row_nnz[blockIdx.x] = kRowToTable;
+    return;
+  }
   const int iu_ax = A == 0 ? 1 : 0, iv_ax = A == 0 ? 2 : 1;
-  const int na = A >= 0 ? g.n[A] : 0;
-  if (A >= 0) {
+  const int na = axis_n(g, A);
+  {
     const int p = sdir > 0 ? 0 : 1;  // the box at the lower coordinate along A
     for (int sl = tid; sl < na; sl += T) {
-      const float c0 = g.o[A] + float(sl) * g.d[A], c1 = g.o[A] + float(sl + 1) * g.d[A];
+      const float c0 = axis_o(g, A) + float(sl) * axis_d(g, A), c1 = axis_o(g, A) + float(sl + 1) * axis_d(g, A);
       int u0, u1, v0, v1;
       slab_window(g, A, box_lo[p], box_hi[p], box_lo[1 - p], box_hi[1 - p], c0, c1, iu_ax, &u0, &u1);
       slab_window(g, A, box_lo[p], box_hi[p], box_lo[1 - p], box_hi[1 - p], c0, c1, iv_ax, &v0, &v1);
@@ -600,15 +656,70 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
       atomicMax(&win_u, u1 - u0 + 1);
       atomicMax(&win_v, v1 - v0 + 1);
     }
-    __syncthreads();
   }
+  __syncthreads();
   const int wu = win_u, wv = win_v;
   const int wuv = wu * wv;
-  bool use_dense = A >= 0 && (long long)na * wuv < (long long)dense_slots(H);  // + the spare slot
-  const int nslots = use_dense ? na * wuv : 0;
+  if (!((long long)na * wuv < (long long)dense_slots(H))) {  // + the spare slot
+    if (tid == 0) row_nnz[blockIdx.x] = kRowToTable;
+    return;
+  }
+  const int nslots = na * wuv;
+  for (int sl = tid; sl < na; sl += T) {
+    const int b = sl * wuv - ulo[sl] * wv - vlo[sl];
+    const int nb = sdir > 0 ? sl + 1 : sl - 1;
+    const int bn = (nb >= 0 && nb < na) ? nb * wuv - ulo[nb] * wv - vlo[nb] : b;
+    sbase[sl] = b;
+    sdk[sl] = bn - b;
+  }
+  for (int i = tid; i <= nslots; i += T) acc[i] = 0.f;
+  __syncthreads();
 
-  const float fr = float(nrays);
-  const size_t base = size_t(blockIdx.x) * H;
+  {
+    auto emit = [&](int ix, int iy, int iz, float L) {
+      const int sa = A == 0 ? ix : iz;
+      const int u = (A == 0 ? iy : ix) - ulo[sa], v = (A == 0 ? iz : iy) - vlo[sa];
+      if (unsigned(u) < unsigned(wu) && unsigned(v) < unsigned(wv))
+        atomicAdd(&acc[sa * wuv + u * wv + v], L);
+      else
+        dense_fail = 1;
+    };
+    // start offsets: the thread index bit-reversed, so that neighbouring
+    // lanes start far apart along the ray
+    const int part = int(__brev(threadIdx.x) >> 24);
+    if (A == 0) {
+      DenseIndex<0> dix{acc, sbase, sdk, wv, nslots};
+      for (int ray = tid; ray < nrays; ray += T) {
+        float r[6];
+        make_ray(ch, seed, cnl, ray, r);
+        if (sdir > 0 ? !(RFSUB(r[3], r[0]) > 0.f) : !(RFSUB(r[3], r[0]) < 0.f)) dense_fail = 1;
+        walk_ray<OISO>(g, ch, r, part, emit, dix, &bad_walk);
+      }
+    } else {
+      DenseIndex<2> dix{acc, sbase, sdk, wv, nslots};
+      for (int ray = tid; ray < nrays; ray += T) {
+        float r[6];
+        make_ray(ch, seed, cnl, ray, r);
+        if (sdir > 0 ? !(RFSUB(r[5], r[2]) > 0.f) : !(RFSUB(r[5], r[2]) < 0.f)) dense_fail = 1;
+        walk_ray<OISO>(g, ch, r, part, emit, dix, &bad_walk);
+      }
+    }
+  }
+  __syncthreads();
+  if (bad_walk) {
+    if (tid == 0) {
+      row_nnz[blockIdx.x] = -1;
+      atomicOr(flags, 2);
+    }
+    return;
+  }
+  // a slot outside the windows was added to the spare slot: every thread
+  // reads the same value and takes the same branch
+  if (dense_fail || acc[nslots] != 0.f) {
+    if (tid == 0) row_nnz[blockIdx.x] = kRowToTable;
+    return;
+  }
+
   // Dense compaction layout: each warp takes a contiguous run of slots
   // (slab-major, then U, then V).
   constexpr int NW = T / 32;
@@ -624,52 +735,131 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
     *y = A == 0 ? iu : iv;
     *z = A == 0 ? iv : sa;
   };
-  for (int pass = 0; pass < 2; pass++) {
-    if (use_dense) {
-      for (int sl = tid; sl < na; sl += T) {
-        const int b = sl * wuv - ulo[sl] * wv - vlo[sl];
-        const int nb = sdir > 0 ? sl + 1 : sl - 1;
-        const int bn = (nb >= 0 && nb < na) ? nb * wuv - ulo[nb] * wv - vlo[nb] : b;
-        sbase[sl] = b;
-        sdk[sl] = bn - b;
+  // First compaction pass: per warp, count the voxels with a positive sum
+  // that pass the cylinder test and clear the others.  A positive slot that
+  // decodes to a voxel outside the grid means the windows missed a voxel:
+  // the row goes to the table kernel.
+  {
+    int cnt = 0;
+    for (int b = b0; b < b1; b += 32) {
+      const int slot = b + lane;
+      bool keep = false;
+      if (slot < b1) {
+        const float v = acc[slot];
+        if (v > 0.f) {
+          int x, y, z;
+          voxel(slot, &x, &y, &z);
+          if (x < g.n[0] && y < g.n[1] && z < g.n[2]) {
+            keep = candidate_test(g, ch, x, y, z);
+          } else {
+            dense_fail = 1;
+          }
+          if (!keep) acc[slot] = 0.f;
+        }
       }
-      for (int i = tid; i <= nslots; i += T) acc[i] = 0.f;
-    } else {
-      for (int i = tid; i < H; i += T) {
-        keys[i] = -1;
-        vals[i] = 0.f;
+      cnt += __popc(__ballot_sync(0xffffffffu, keep));
+    }
+    if (lane == 0) warp_sums[w] = cnt;
+  }
+  __syncthreads();
+  if (dense_fail) {
+    if (tid == 0) row_nnz[blockIdx.x] = kRowToTable;
+    return;
+  }
+  // Second pass: after a scan of the warp counts, each warp writes its
+  // voxels in slot order -- column order for x slabs; z slabs are sorted
+  // below.
+  const float fr = float(nrays);
+  const size_t base = size_t(blockIdx.x) * H;
+  int before = 0, total = 0;
+  for (int k = 0; k < NW; k++) {
+    const int c = warp_sums[k];
+    before += k < w ? c : 0;
+    total += c;
+  }
+  if (total > H) {
+    if (tid == 0) {
+      row_nnz[blockIdx.x] = -1;
+      atomicOr(flags, 1);
+    }
+    return;
+  }
+  for (int b = b0; b < b1; b += 32) {
+    const int slot = b + lane;
+    const bool keep = slot < b1 && acc[slot] > 0.f;
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const int pos = before + __popc(m & ((1u << lane) - 1u));
+      int x, y, z;
+      voxel(slot, &x, &y, &z);
+      st_col[base + pos] = x * nyz + y * nz + z;
+      st_val[base + pos] = RFDIV(acc[slot], fr);
+    }
+    before += __popc(m);
+  }
+  if (A == 0) {
+    if (tid == 0) row_nnz[blockIdx.x] = total;
+    return;
+  }
+  __syncthreads();
+  for (int i = tid; i < total; i += T) {
+    keys[i] = st_col[base + i];
+    vals[i] = st_val[base + i];
+  }
+  sort_and_write<T>(keys, vals, total, st_col, st_val, base, row_nnz + blockIdx.x);
+}
+
+// Table kernel: its rays (generated, or given in `rays`) summed per voxel in
+// an open-addressing hash table of H keys in shared memory, then the voxels
+// with a positive sum that pass the cylinder test sorted into column order.
+// Each CTA takes rows blockIdx.x, blockIdx.x + gridDim.x, ... of the nrows.
+// With only_flagged it builds only the rows the dense kernel left with
+// kRowToTable and leaves the others alone (launched then with a small grid:
+// most workloads leave none, and the blocks only read the row states).
+template <int H, int T, bool OISO>
+__global__ void __launch_bounds__(T) sm_table_kernel(DGeom g, const float2* __restrict__ sincos,
+                                                     const int32_t* __restrict__ cnl_ids, int64_t row0, int64_t nrows,
+                                                     int nrays, uint32_t seed, const float* __restrict__ rays,
+                                                     int32_t* __restrict__ st_col, float* __restrict__ st_val,
+                                                     int32_t* __restrict__ row_nnz, int32_t* __restrict__ flags,
+                                                     int only_flagged) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int* keys = reinterpret_cast<int*>(smem);
+  float* vals = reinterpret_cast<float*>(smem + H * sizeof(int));
+  __shared__ Channel ch;
+  __shared__ int overflow, bad_walk;
+  __shared__ int warp_sums[32];
+
+  const int tid = threadIdx.x;
+  const int nyz = g.n[1] * g.n[2];
+  const int nz = g.n[2];
+  for (int64_t bi = blockIdx.x; bi < nrows; bi += gridDim.x) {
+    if (only_flagged && row_nnz[bi] != kRowToTable) continue;
+    const int64_t li = row0 + bi;
+    const int cnl = cnl_ids[li];
+    if (cnl < 0 || cnl >= num_channels(g)) {
+      if (tid == 0) {
+        row_nnz[bi] = -1;
+        atomicOr(flags, 4);
       }
+      continue;
+    }
+    __syncthreads();  // the previous row's use of the shared memory is over
+    if (tid == 0) {
+      channel_setup(g, sincos, cnl, ch);
+      overflow = 0;
+      bad_walk = 0;
+    }
+    for (int i = tid; i < H; i += T) {
+      keys[i] = -1;
+      vals[i] = 0.f;
     }
     __syncthreads();
-
-    if (use_dense) {
-      auto emit = [&](int ix, int iy, int iz, float L) {
-        const int sa = A == 0 ? ix : iz;
-        const int u = (A == 0 ? iy : ix) - ulo[sa], v = (A == 0 ? iz : iy) - vlo[sa];
-        if (unsigned(u) < unsigned(wu) && unsigned(v) < unsigned(wv))
-          atomicAdd(&acc[sa * wuv + u * wv + v], L);
-        else
-          dense_fail = 1;
-      };
-      DenseIndex<0> dix0{acc, sbase, sdk, wv, nslots};
-      DenseIndex<2> dix2{acc, sbase, sdk, wv, nslots};
-      for (int ray = tid; ray < nrays; ray += T) {
-        float r[6];
-        make_ray(ch, seed, cnl, ray, r);
-        const float da = A == 0 ? RFSUB(r[3], r[0]) : RFSUB(r[5], r[2]);
-        if (sdir > 0 ? !(da > 0.f) : !(da < 0.f)) dense_fail = 1;
-        // start offsets: the thread index bit-reversed, so that neighbouring
-        // lanes start far apart along the ray
-        const int part = int(__brev(threadIdx.x) >> 24);
-        if (A == 0)
-          walk_ray<OISO>(g, ch, r, part, emit, dix0, &bad_walk);
-        else
-          walk_ray<OISO>(g, ch, r, part, emit, dix2, &bad_walk);
-      }
-    } else {
+    {
       RowTable<H> table{keys, vals, &overflow};
       KeyIndex<H> kix{&table, nyz, nz};
       auto emit = [&](int ix, int iy, int iz, float L) { table.add(ix * nyz + iy * nz + iz, L); };
+      const int part = int(__brev(threadIdx.x) >> 24);
       for (int ray = tid; ray < nrays; ray += T) {
         float r[6];
         if (rays) {
@@ -679,96 +869,19 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
         } else {
           make_ray(ch, seed, cnl, ray, r);
         }
-        walk_ray<OISO>(g, ch, r, int(__brev(threadIdx.x) >> 24), emit, kix, &bad_walk);
+        walk_ray<OISO>(g, ch, r, part, emit, kix, &bad_walk);
       }
     }
     __syncthreads();
-    // a slot outside the windows was added to the spare slot: every thread
-    // reads the same value and takes the same branch
-    const bool spare = use_dense && acc[nslots] != 0.f;
-    if (use_dense && !dense_fail && !bad_walk && !spare) {
-      // First compaction pass: per warp, count the voxels with a positive
-      // sum that pass the cylinder test and clear the others.  A positive
-      // slot that decodes to a voxel outside the grid means the windows
-      // missed a voxel: the row is redone with the table.
-      int cnt = 0;
-      for (int b = b0; b < b1; b += 32) {
-        const int slot = b + lane;
-        bool keep = false;
-        if (slot < b1) {
-          const float v = acc[slot];
-          if (v > 0.f) {
-            int x, y, z;
-            voxel(slot, &x, &y, &z);
-            if (x < g.n[0] && y < g.n[1] && z < g.n[2]) {
-              keep = candidate_test(g, ch, x, y, z);
-            } else {
-              dense_fail = 1;
-            }
-            if (!keep) acc[slot] = 0.f;
-          }
-        }
-        cnt += __popc(__ballot_sync(0xffffffffu, keep));
-      }
-      if (lane == 0) warp_sums[w] = cnt;
-      __syncthreads();
-    }
-    if (!(use_dense && (dense_fail || spare))) break;
-    use_dense = false;  // redo the row with the table
-    __syncthreads();
-  }
-
-  if (overflow || bad_walk) {
-    if (tid == 0) {
-      row_nnz[blockIdx.x] = -1;
-      atomicOr(flags, overflow ? 1 : 2);
-    }
-    return;
-  }
-
-  int total = 0;
-  if (use_dense) {
-    // Second pass: after a scan of the warp counts, each warp writes its
-    // voxels in slot order -- column order for x slabs; z slabs are sorted
-    // below.
-    int before = 0;
-    for (int k = 0; k < NW; k++) {
-      const int c = warp_sums[k];
-      before += k < w ? c : 0;
-      total += c;
-    }
-    if (total > H) {
+    if (overflow || bad_walk) {
       if (tid == 0) {
-        row_nnz[blockIdx.x] = -1;
-        atomicOr(flags, 1);
+        row_nnz[bi] = -1;
+        atomicOr(flags, overflow ? 1 : 2);
       }
-      return;
+      continue;
     }
-    for (int b = b0; b < b1; b += 32) {
-      const int slot = b + lane;
-      const bool keep = slot < b1 && acc[slot] > 0.f;
-      const unsigned m = __ballot_sync(0xffffffffu, keep);
-      if (keep) {
-        const int pos = before + __popc(m & ((1u << lane) - 1u));
-        int x, y, z;
-        voxel(slot, &x, &y, &z);
-        st_col[base + pos] = x * nyz + y * nz + z;
-        st_val[base + pos] = RFDIV(acc[slot], fr);
-      }
-      before += __popc(m);
-    }
-    if (A == 0) {
-      if (tid == 0) row_nnz[blockIdx.x] = total;
-      return;
-    }
-    __syncthreads();
-    for (int i = tid; i < total; i += T) {
-      keys[i] = st_col[base + i];
-      vals[i] = st_val[base + i];
-    }
-  } else {
-    // Compaction: keep voxels with a positive sum that pass the cylinder
-    // test.
+    // Compaction: keep voxels with a positive sum that pass the cylinder test.
+    const float fr = float(nrays);
     constexpr int PER = H / T;
     int kr[PER];
     float vr[PER];
@@ -790,6 +903,7 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
       vr[j] = ok ? RFDIV(v, fr) : 0.f;
       cnt += ok ? 1 : 0;
     }
+    int total = 0;
     int pos = block_exclusive_scan<T>(cnt, &total, warp_sums);
 #pragma unroll
     for (int j = 0; j < PER; j++) {
@@ -799,37 +913,8 @@ __global__ void __launch_bounds__(T) sm_rows_kernel(DGeom g, const float2* __res
         pos++;
       }
     }
+    sort_and_write<T>(keys, vals, total, st_col, st_val, size_t(bi) * H, row_nnz + bi);
   }
-  int npad = 1;
-  while (npad < total) npad <<= 1;
-  for (int i = total + tid; i < npad; i += T) keys[i] = INT_MAX;
-  __syncthreads();
-
-  // Bitonic sort of (key, value) by key over [0, npad).
-  for (int k = 2; k <= npad; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int t = tid; t < (npad >> 1); t += T) {
-        int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
-        int p = i | j;
-        bool asc = (i & k) == 0;
-        int ki = keys[i], kp = keys[p];
-        if ((ki > kp) == asc) {
-          keys[i] = kp;
-          keys[p] = ki;
-          float vi = vals[i];
-          vals[i] = vals[p];
-          vals[p] = vi;
-        }
-      }
-      __syncthreads();
-    }
-  }
-
-  for (int i = tid; i < total; i += T) {
-    st_col[base + i] = keys[i];
-    st_val[base + i] = vals[i];
-  }
-  if (tid == 0) row_nnz[blockIdx.x] = total;
 }
 
 struct Level {
@@ -842,16 +927,32 @@ template <int H, int T>
 cudaError_t launch_level(const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0, int64_t nrows,
                          int nrays, uint32_t seed, const float* d_rays, int32_t* st_col, float* st_val,
                          int32_t* row_nnz, int32_t* d_flags, cudaStream_t s) {
-  const size_t smem = row_smem_bytes(H);
   // A grid with the same origin on every axis (the usual centred cube) lets
   // the walk's step skip selecting the origin.
   const bool oiso = g.o[0] == g.o[1] && g.o[1] == g.o[2];
-  auto kern = oiso ? sm_rows_kernel<H, T, true> : sm_rows_kernel<H, T, false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  auto table = oiso ? sm_table_kernel<H, T, true> : sm_table_kernel<H, T, false>;
+  const size_t table_smem = size_t(H) * 8;
+  cudaError_t e = cudaFuncSetAttribute(table, cudaFuncAttributeMaxDynamicSharedMemorySize, int(table_smem));
   if (e != cudaSuccess) return e;
-  kern<<<unsigned(nrows), T, smem, s>>>(g, d_sincos, d_cnl, row0, nrays, seed, d_rays, st_col, st_val, row_nnz,
-                                        d_flags);
-  note_launches(1);
+  if (d_rays) {
+    // caller-supplied rays: the table builds every row, one CTA each
+    table<<<unsigned(nrows), T, table_smem, s>>>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col,
+                                                  st_val, row_nnz, d_flags, 0);
+    note_launches(1);
+    return cudaGetLastError();
+  }
+  auto dense = oiso ? sm_dense_kernel<H, T, true> : sm_dense_kernel<H, T, false>;
+  const size_t dense_smem = row_smem_bytes(H);
+  e = cudaFuncSetAttribute(dense, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dense_smem));
+  if (e != cudaSuccess) return e;
+  dense<<<unsigned(nrows), T, dense_smem, s>>>(g, d_sincos, d_cnl, row0, nrays, seed, st_col, st_val, row_nnz,
+                                               d_flags);
+  // the rows the dense kernel left to the table (none on most workloads),
+  // four blocks per SM looking through the row states
+  const int64_t tb = std::min<int64_t>(nrows, 148 * 4);
+  table<<<unsigned(tb), T, table_smem, s>>>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, nullptr, st_col, st_val,
+                                            row_nnz, d_flags, 1);
+  note_launches(2);
   return cudaGetLastError();
 }
 

@@ -146,10 +146,22 @@ struct Entry {
   raptr_status launch_status = RAPTR_OK;
   std::string launch_error;
   std::vector<Request*> members;
-  float* X = nullptr;
+  // The batch's interleaved arrays, allocated for kcap frames and reused
+  // while the batch changes (grown, never shrunk): images in two buffers
+  // (a relayout reads one and writes the other), measurements in one (they
+  // are rebuilt from the requests' own vectors), and the small index
+  // arrays of a relayout, staged through page-locked host memory.
+  float* Xbuf[2] = {nullptr, nullptr};
+  int xcur = 0;
   float* Y = nullptr;
-  int K = 0;
-  int64_t batch_bytes() const { return int64_t(K) * (m + n) * int64_t(sizeof(float)); }
+  float* tmp = nullptr;  // one image, for a finished request's copy to the host
+  int* d_src = nullptr;
+  const float** d_ys = nullptr;
+  int* h_src = nullptr;
+  const float** h_ys = nullptr;
+  int K = 0, kcap = 0;
+  float* X() const { return Xbuf[xcur]; }
+  int64_t batch_bytes() const { return int64_t(kcap) * (2 * n + m) * int64_t(sizeof(float)); }
 };
 
 }  // namespace
@@ -261,63 +273,100 @@ raptr_status raptr_server::build(Entry* e, std::string* err) {
 void raptr_server::drop(Entry* e) {
   DeviceScope ds(device);
   if (e->stream) cudaStreamSynchronize(e->stream);
-  cudaFree(e->X);
+  cudaFree(e->Xbuf[0]);
+  cudaFree(e->Xbuf[1]);
   cudaFree(e->Y);
+  cudaFree(e->tmp);
+  cudaFree(e->d_src);
+  cudaFree(e->d_ys);
+  cudaFreeHost(e->h_src);
+  cudaFreeHost(e->h_ys);
+  e->Xbuf[0] = e->Xbuf[1] = e->tmp = nullptr;
+  e->d_src = nullptr;
+  e->d_ys = nullptr;
+  e->h_src = nullptr;
+  e->h_ys = nullptr;
+  e->kcap = e->K = 0;
   cudaFree(e->s);
   if (e->A) raptr_matrix_destroy(e->A);
   if (e->ctx) raptr_ctx_destroy(e->ctx);
   if (e->stream) cudaStreamDestroy(e->stream);
   if (e->done_ev) cudaEventDestroy(e->done_ev);
   e->done_ev = nullptr;
-  e->X = e->Y = e->s = nullptr;
+  e->Y = e->s = nullptr;
   e->A = nullptr;
   e->ctx = nullptr;
   e->stream = nullptr;
 }
 
-// New interleaved arrays for the batch's current requests: K = the next
-// power of two >= 4 that holds them; padding slots repeat slot 0.
+// Lays the batch out again for its current requests: K = the smallest
+// multiple of 4 that holds them (the batch kernels run any such K in tiles
+// of at most 32 frames, so at most 3 slots are padding, which repeat slot
+// 0).  The arrays are reused; only a batch that outgrows them allocates
+// (the next power of two of frames, up to max_frames), so requests joining
+// and leaving do not allocate or synchronise.
 cudaError_t raptr_server::relayout(Entry* e) {
   const int cnt = int(e->active.size());
-  int K = 4;
-  while (K < cnt) K <<= 1;
-  std::vector<int> src(static_cast<size_t>(K));
-  std::vector<const float*> ys(static_cast<size_t>(K));
+  const int K = std::max(4, (cnt + 3) & ~3);
+  cudaError_t ce = cudaSuccess;
+  if (!e->h_src) {
+    ce = cudaMallocHost(&e->h_src, 64 * sizeof(int));
+    if (ce == cudaSuccess) ce = cudaMallocHost(&e->h_ys, 64 * sizeof(float*));
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->d_src, 64 * sizeof(int));
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->d_ys, 64 * sizeof(float*));
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->tmp, size_t(e->n) * sizeof(float));
+    if (ce != cudaSuccess) return ce;
+  }
   for (int s = 0; s < K; s++) {
     Request* r = e->active[size_t(s < cnt ? s : 0)];
-    src[size_t(s)] = (r->slot >= 0 && e->X) ? r->slot : -1;
-    ys[size_t(s)] = r->y_dev;
+    e->h_src[s] = (r->slot >= 0 && e->X()) ? r->slot : -1;
+    e->h_ys[s] = r->y_dev;
   }
-  float *X = nullptr, *Y = nullptr;
-  int* d_src = nullptr;
-  const float** d_ys = nullptr;
-  cudaError_t ce = cudaMalloc(&X, size_t(e->n) * K * sizeof(float));
-  if (ce == cudaSuccess) ce = cudaMalloc(&Y, size_t(std::max<int64_t>(e->m, 1)) * K * sizeof(float));
-  if (ce == cudaSuccess) ce = cudaMalloc(&d_src, size_t(K) * sizeof(int));
-  if (ce == cudaSuccess) ce = cudaMalloc(&d_ys, size_t(K) * sizeof(float*));
+  float* from = e->X();
+  float* to = e->Xbuf[1 - e->xcur];
+  float* old_other = nullptr;
+  float* old_cur = nullptr;
+  if (K > e->kcap) {
+    int kc = 4;
+    while (kc < K) kc <<= 1;
+    kc = std::min(kc, std::max(K, int(opts.max_frames + 3) & ~3));
+    float *x0 = nullptr, *x1 = nullptr, *y = nullptr;
+    ce = cudaMalloc(&x0, size_t(e->n) * kc * sizeof(float));
+    if (ce == cudaSuccess) ce = cudaMalloc(&x1, size_t(e->n) * kc * sizeof(float));
+    if (ce == cudaSuccess) ce = cudaMalloc(&y, size_t(std::max<int64_t>(e->m, 1)) * kc * sizeof(float));
+    if (ce != cudaSuccess) {
+      cudaFree(x0);
+      cudaFree(x1);
+      cudaFree(y);
+      return ce;
+    }
+    old_cur = e->Xbuf[e->xcur];
+    old_other = e->Xbuf[1 - e->xcur];
+    cudaFree(e->Y);  // rebuilt from the requests' vectors below
+    e->Xbuf[1 - e->xcur] = x0;
+    e->Xbuf[e->xcur] = x1;
+    e->Y = y;
+    e->kcap = kc;
+    to = x0;
+  }
+  ce = cudaMemcpyAsync(e->d_src, e->h_src, size_t(K) * sizeof(int), cudaMemcpyHostToDevice, e->stream);
   if (ce == cudaSuccess)
-    ce = cudaMemcpyAsync(d_src, src.data(), size_t(K) * sizeof(int), cudaMemcpyHostToDevice, e->stream);
-  if (ce == cudaSuccess)
-    ce = cudaMemcpyAsync(d_ys, ys.data(), size_t(K) * sizeof(float*), cudaMemcpyHostToDevice, e->stream);
+    ce = cudaMemcpyAsync(e->d_ys, e->h_ys, size_t(K) * sizeof(float*), cudaMemcpyHostToDevice, e->stream);
   if (ce == cudaSuccess) {
-    frames_relayout_kernel<<<grid_of(e->n * K), 256, 0, e->stream>>>(e->n, e->K, e->X, K, d_src,
-                                                                     float(1.0 / double(e->n)), X);
-    frames_from_vectors_kernel<<<grid_of(e->m * K), 256, 0, e->stream>>>(e->m, K, d_ys, Y);
+    frames_relayout_kernel<<<grid_of(e->n * K), 256, 0, e->stream>>>(e->n, e->K, from, K, e->d_src,
+                                                                     float(1.0 / double(e->n)), to);
+    frames_from_vectors_kernel<<<grid_of(e->m * K), 256, 0, e->stream>>>(e->m, K, e->d_ys, e->Y);
     note_launches(2);
     ce = cudaGetLastError();
   }
-  if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
-  cudaFree(d_src);
-  cudaFree(d_ys);
-  if (ce != cudaSuccess) {
-    cudaFree(X);
-    cudaFree(Y);
-    return ce;
+  if (old_cur || old_other) {
+    // the relayout above read the old image buffer: free it after that
+    cudaStreamSynchronize(e->stream);
+    cudaFree(old_cur);
+    cudaFree(old_other);
   }
-  cudaFree(e->X);
-  cudaFree(e->Y);
-  e->X = X;
-  e->Y = Y;
+  if (ce != cudaSuccess) return ce;
+  e->xcur = (to == e->Xbuf[0]) ? 0 : 1;
   e->K = K;
   for (int s = 0; s < cnt; s++) {
     e->active[size_t(s)]->slot = s;
@@ -391,16 +440,17 @@ bool raptr_server::admit(std::unique_lock<std::mutex>& lk) {
       it = std::find(queue.begin(), queue.end(), r);
       if (it == queue.end()) break;
     }
-    // measurement on the device
+    // measurement on the device (stream-ordered allocation: no device-wide
+    // synchronisation while other batches run)
     DeviceScope ds(device);
-    cudaError_t ce = cudaMalloc(&r->y_dev, size_t(e->m) * sizeof(float));
+    cudaError_t ce = cudaMallocAsync(&r->y_dev, size_t(e->m) * sizeof(float), e->stream);
     if (ce == cudaSuccess)
       ce = cudaMemcpyAsync(r->y_dev, r->y_host.data(), size_t(e->m) * sizeof(float), cudaMemcpyHostToDevice,
                            e->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
     if (ce != cudaSuccess) {
       (void)cudaGetLastError();
-      cudaFree(r->y_dev);
+      if (r->y_dev) cudaFreeAsync(r->y_dev, e->stream);
       r->y_dev = nullptr;
       break;  // retry when memory frees up
     }
@@ -446,9 +496,9 @@ void raptr_server::loop() {
         e->launch_status = RAPTR_ERR_NOMEM;
         e->launch_error = "batch relayout failed";
       } else {
-        // one sweep of the matrix for all frames (K is a power of two <= 64)
+        // all frames in sweeps of at most 32 (a multiple of 4 frames)
         e->launch_status = raptr_mlem_batch(e->ctx, e->m, e->n, e->K, 1, e->rp, e->col, e->hval, e->rscale, e->cp,
-                                            e->trow, e->htval, e->rank, e->Y, e->s, e->X, 1, e->K, nullptr,
+                                            e->trow, e->htval, e->rank, e->Y, e->s, e->X(), 1, 32, nullptr,
                                             e->stream);
         if (e->launch_status != RAPTR_OK) e->launch_error = raptr_last_error();
       }
@@ -468,18 +518,15 @@ void raptr_server::loop() {
         ended.push_back(e);
         finished.emplace_back();
         if (e->launch_status != RAPTR_OK) continue;
-        float* tmp = nullptr;
         for (Request* r : e->members) {
           if (r->done + 1 < r->n_iter) continue;
-          if (!tmp && cudaMalloc(&tmp, size_t(e->n) * sizeof(float)) != cudaSuccess) break;
           std::vector<float> x(size_t(e->n));
-          frame_extract_kernel<<<grid_of(e->n), 256, 0, e->stream>>>(e->n, e->K, r->slot, e->X, tmp);
+          frame_extract_kernel<<<grid_of(e->n), 256, 0, e->stream>>>(e->n, e->K, r->slot, e->X(), e->tmp);
           note_launches(1);
-          cudaMemcpyAsync(x.data(), tmp, size_t(e->n) * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
+          cudaMemcpyAsync(x.data(), e->tmp, size_t(e->n) * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
           cudaStreamSynchronize(e->stream);
           finished.back().emplace_back(r, std::move(x));
         }
-        cudaFree(tmp);
       }
     }
     if (ended.empty()) {
@@ -495,7 +542,7 @@ void raptr_server::loop() {
       if (e->launch_status != RAPTR_OK) {
         for (Request* r : e->members) {
           if (r->state != 1) continue;
-          cudaFree(r->y_dev);
+          cudaFreeAsync(r->y_dev, e->stream);
           r->y_dev = nullptr;
           state_bytes -= e->m * 4;
           cache.unpin(r->key);
@@ -510,7 +557,7 @@ void raptr_server::loop() {
           r->x_host = std::move(f.second);
           r->state = 2;
           r->t_done = Clock::now();
-          cudaFree(r->y_dev);
+          cudaFreeAsync(r->y_dev, e->stream);
           r->y_dev = nullptr;
           state_bytes -= e->m * 4;
           cache.unpin(r->key);

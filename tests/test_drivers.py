@@ -1,7 +1,7 @@
 """The command-line drivers with the reference's argv (reco,
 backprojection, pureSMCalculation): argument and file errors on the host;
-on the GPU, their outputs equal the library's Python path on the same
-files."""
+on the GPU, their output files match the CPU oracle on the same
+geometry, rays and measurement."""
 import os
 import subprocess
 
@@ -55,55 +55,62 @@ def grid_geometry(path):
 
 
 @pytest.mark.gpu
-def test_reco_backprojection_and_build_match_python(rlib, drivers, tmp_path):
-    import torch
-
+def test_reco_backprojection_and_build_match_the_oracle(rlib, oracle, drivers, tmp_path):
+    """The drivers' files against the CPU oracle on the same geometry and
+    rays: reco's density after every iteration ("<it>_<output>",
+    src/tests/reco.cu:305-311) against the oracle's MLEM over the measured
+    rows (src/tests/reco.cu:229-321), backprojection's normalised A^T y
+    (src/tests/backprojection.cu:156-189) against the oracle's transposed
+    CSRmv, and pureSMCalculation's entry count against the oracle's rows."""
     g0 = cfg.SMALL
     nrays = 40
-    # sensitivity of all channels and a measurement, as the library computes them
-    ctx = rlib.Context(g0, 0)
-    A_all = ctx.build(np.arange(g0.n_channels, dtype=np.int32), nrays, 1251)
-    s64, s32 = rlib.sensitivity(A_all)
+    # the grid the drivers read from the sensitivity file's attributes
     sfile = str(tmp_path / "sens.h5")
-    h5.write_density(sfile, s64.float().cpu().numpy(), g0)
+    h5.write_density(sfile, np.ones(g0.n_voxels, np.float32), g0)
     g = grid_geometry(sfile)
-    ctx = rlib.Context(g, 0)
-    A_all = ctx.build(np.arange(g.n_channels, dtype=np.int32), nrays, 1251)
-    lam = rlib.spmv(rlib.OP_N, A_all.m, A_all.n, A_all.row_ptr, A_all.col, A_all.val,
-                    torch.from_numpy(cfg.phantom(g, rods=False)).cuda()).cpu().numpy()
-    y = cfg.poisson_measurement(lam, 1e5, 11)
+    # a measurement of 6000 random channels, Poisson counts of the oracle's rows
+    rng = np.random.default_rng(5)
+    cand = np.sort(rng.choice(g.n_channels, 6000, replace=False)).astype(np.int32)
+    rp_c, col_c, val_c = oracle.sysmat(g, cand, nrays, 1251, method=1)
+    lam = oracle.spmv(0, cand.size, g.n_voxels, rp_c, col_c, val_c, cfg.phantom(g, rods=False).astype(np.float64),
+                      dtype=np.float64)
+    yc = cfg.poisson_measurement(lam, 2e5, 11)
+    y = np.zeros(g.n_channels, np.float32)
+    y[cand] = yc
+    rows = np.nonzero(y)[0].astype(np.int32)
+    rp, col, val = oracle.sysmat(g, rows, nrays, 1251, method=1)
+    m, n = rows.size, g.n_voxels
+    # sensitivity: FP64 column sums of the measured rows, written as the
+    # file reco reads
+    s64 = oracle.column_sums_f64(m, n, rp, col, val)
+    h5.write_density(sfile, s64.astype(np.float32), g0)  # the same grid attributes as before
+    assert grid_geometry(sfile) == g
     mfile = str(tmp_path / "meas.h5")
     h5.write_measurement(mfile, y, g)
     env = {"RAPTR_SETUP": SETUP, "RAPTR_GRID": "{},{},{},{},{},{},{},{},{}".format(*g.grid_n, *g.grid_o, *g.grid_d)}
 
-    # reco: 3 iterations from a missing guess (all ones), outputs per iteration
+    # reco: 3 iterations from a missing guess (all ones), one file per iteration
     out = str(tmp_path / "out.h5")
     r = run(drivers["reco"], mfile, out, nrays, sfile, 3, str(tmp_path / "none.h5"), env=env)
     assert r.returncode == 0, r.stderr + r.stdout
-    rows = np.nonzero(y)[0].astype(np.int32)
-    A = ctx.build(rows, nrays, 1251)
-    A.transpose()
-    s = torch.from_numpy(h5.read_density(sfile)[0].ravel()).cuda()
-    s = s / s.sum()
-    x = torch.ones(g.n_voxels, device="cuda")
-    yd = torch.from_numpy(y[rows]).cuda()
+    sf = h5.read_density(sfile)[0].ravel()
+    s = (sf / np.float32(sf.astype(np.float64).sum())).astype(np.float32)
     for it in range(3):
-        ctx.mlem(A, yd, s, x, 1, use_graph=False)
+        want = oracle.mlem(m, n, rp, col, val, y[rows], s, np.ones(n, np.float32), it + 1)
         d, grid = h5.read_density(str(tmp_path / f"{it}_out.h5"))
         assert grid["n"] == tuple(g.grid_n)
-        want = x.cpu().numpy()
-        assert np.linalg.norm(d.ravel() - want) / np.linalg.norm(want) < 1e-6
+        assert np.linalg.norm(d.ravel() - want) / np.linalg.norm(want) < 1e-4
 
-    # backprojection: normalised A^T y
+    # backprojection: A^T y normalised to sum 1
     bout = str(tmp_path / "bp.h5")
     r = run(drivers["backprojection"], mfile, bout, nrays, env=env)
     assert r.returncode == 0, r.stderr
-    bp = rlib.spmv(rlib.OP_T, A.m, A.n, A.row_ptr, A.col, A.val, yd).cpu().numpy()
+    bp = oracle.spmv(1, m, n, rp, col, val, y[rows].astype(np.float64), dtype=np.float64)
     bp = bp / bp.sum()
     d, _ = h5.read_density(bout)
     assert np.linalg.norm(d.ravel() - bp) / np.linalg.norm(bp) < 1e-5
 
-    # pureSMCalculation: the same number of entries
+    # pureSMCalculation: the oracle's number of entries
     r = run(drivers["pureSMCalculation"], mfile, nrays, env=env)
     assert r.returncode == 0, r.stderr
-    assert f"entries {A.nnz}," in r.stdout
+    assert f"entries {int(rp[-1])}," in r.stdout

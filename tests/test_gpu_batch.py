@@ -75,7 +75,7 @@ def test_batch_graph_timing_and_autotune(rlib, torch, frames):
     Yd = torch.from_numpy(Y).cuda()
     X0 = torch.full((n, K), np.float32(1.0 / n), device="cuda")
     best, ms = ctx.batch_autotune(A, Yd, s, X0)
-    assert best in ms and set(ms) == {4, 8}
+    assert best in ms and set(ms) == {4, 8, 16, 32, 64}
     assert torch.all(X0 == np.float32(1.0 / n))  # the autotuner leaves the images alone
     Xg = X0.clone()
     ctx.mlem_batch(A, Yd, s, Xg, 3, frame_tile=best, use_graph=True)
@@ -91,9 +91,10 @@ def test_batch_rejects_bad_tile(rlib, torch, frames):
     s = rlib.sensitivity(A)[1]
     X = torch.full((n, K), np.float32(1.0 / n), device="cuda")
     with pytest.raises(RuntimeError):
-        ctx.mlem_batch(A, torch.from_numpy(Y).cuda(), s, X, 1, frame_tile=16)  # does not divide 8
-    with pytest.raises(RuntimeError):
         ctx.mlem_batch(A, torch.from_numpy(Y).cuda(), s, X, 1, frame_tile=6)
+    X6 = torch.full((n, 6), np.float32(1.0 / n), device="cuda")
+    with pytest.raises(RuntimeError):  # not a multiple of 4 frames
+        ctx.mlem_batch(A, torch.from_numpy(np.ascontiguousarray(Y[:, :6])).cuda(), s, X6, 1, frame_tile=4)
 
 
 # ---------------------------------------------------------------- 64 frames
