@@ -12,10 +12,10 @@
 // dataspace, a floating-point or fixed-point datatype, a fill-value message
 // and a contiguous version-3 layout, and version-1 attribute messages.
 //
-// The reader walks the same structures (also header continuation blocks)
-// and reads contiguous float32/float64 and int32 datasets; other layouts
-// (chunked, compressed) and other superblock versions are reported as
-// unsupported.
+// The reader walks these structures and also the later forms libhdf5 and
+// h5py write with their latest-format settings and for chunked datasets
+// (see "reading" below).
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -297,6 +297,26 @@ int write_file(const char* path, const char* name, const float* data, const std:
 }
 
 // ---- reading ------------------------------------------------------------------
+//
+// The reader follows the HDF5 file format specification (version 3.0) for
+// the forms libhdf5 and h5py write for these files, in their default and
+// in their latest-format settings:
+//   * superblock versions 0 and 1 (root group as a symbol table) and 2 and 3
+//     (root group object header address), 8-byte offsets and lengths;
+//   * object headers of version 1 and 2 ("OHDR", continuation blocks
+//     "OCHK"); checksums are not verified;
+//   * groups held by a symbol table (version-1 B-tree, "SNOD" nodes, local
+//     heap) or by link messages in the header (compact storage);
+//   * dataspace messages of version 1 and 2, datatype messages of versions
+//     1-4 (little-endian float32, float64, int32), attribute messages of
+//     version 1, 2 and 3 stored in the header;
+//   * data layout messages of version 3 and 4: contiguous data; chunked
+//     data indexed by a version-1 B-tree (layout version 3) or, in layout
+//     version 4, by the single-chunk, implicit or (unpaged) fixed-array
+//     index -- without filters (a filter pipeline means compressed data).
+// Other forms (dense link or attribute storage in fractal heaps, extensible
+// arrays and version-2 B-trees as chunk indexes, paged fixed arrays,
+// filters) are reported as unsupported.
 
 struct File {
   std::vector<uint8_t> b;
@@ -305,6 +325,12 @@ struct File {
   T get(uint64_t at) const {
     T v{};
     std::memcpy(&v, &b[at], sizeof(T));
+    return v;
+  }
+  // little-endian unsigned integer of n bytes (1..8)
+  uint64_t getn(uint64_t at, int n) const {
+    uint64_t v = 0;
+    for (int i = n - 1; i >= 0; i--) v = (v << 8) | b[at + uint64_t(i)];
     return v;
   }
 };
@@ -316,8 +342,20 @@ struct Dataset {
   bool big_endian = false;
   bool is_signed = true;
   uint64_t addr = kUndef, nbytes = 0;
-  int layout = -1;
+  int layout = -1;          // 1 contiguous, 2 chunked
+  int layout_version = 0;
+  std::vector<uint64_t> chunk;  // chunk dimensions in elements (rank entries)
+  int index_type = 0;       // layout 4: 1 single chunk, 2 implicit, 3 fixed array; layout 3: B-tree (0)
+  bool filtered = false;    // a filter pipeline message is present
   std::map<std::string, double> attrs;
+};
+
+// What an object header holds for a group: a symbol table, links, or dense
+// link storage (not read).
+struct GroupInfo {
+  uint64_t btree = kUndef, heap = kUndef;
+  std::map<std::string, uint64_t> links;
+  bool dense_links = false;
 };
 
 bool parse_dtype(const File& f, uint64_t at, uint64_t len, int* cls, uint32_t* size, bool* be, bool* sg) {
@@ -331,7 +369,7 @@ bool parse_dtype(const File& f, uint64_t at, uint64_t len, int* cls, uint32_t* s
 }
 
 bool parse_dataspace(const File& f, uint64_t at, uint64_t len, std::vector<uint64_t>* dims) {
-  if (len < 8 || !f.ok(at, len)) return false;
+  if (len < 4 || !f.ok(at, len)) return false;
   const int ver = f.b[at], rank = f.b[at + 1];
   uint64_t p = at + (ver == 1 ? 8 : 4);
   dims->clear();
@@ -352,66 +390,172 @@ double scalar_value(const File& f, uint64_t at, int cls, uint32_t size, bool be)
   return 0.0;
 }
 
-// Messages of a version-1 object header (following continuation blocks).
-bool parse_object(const File& f, uint64_t oh, Dataset* ds, uint64_t* btree, uint64_t* heap) {
-  if (!f.ok(oh, 16) || f.b[oh] != 1) return false;
-  const int nmsg = f.get<uint16_t>(oh + 2);
+// Attribute message (versions 1-3) holding a scalar or one-element value.
+void parse_attribute(const File& f, uint64_t body, uint64_t len, Dataset* ds) {
+  if (len < 8 || !f.ok(body, len)) return;
+  const int ver = f.b[body];
+  if (ver < 1 || ver > 3) return;
+  const uint16_t nlen = f.get<uint16_t>(body + 2), tlen = f.get<uint16_t>(body + 4), slen = f.get<uint16_t>(body + 6);
+  uint64_t q = body + 8 + (ver == 3 ? 1 : 0);  // version 3: character set of the name
+  auto step = [&](uint64_t n) { return ver == 1 ? up8(n) : n; };  // version 1 pads to 8 bytes
+  if (!f.ok(q, nlen)) return;
+  std::string an(reinterpret_cast<const char*>(&f.b[q]), strnlen(reinterpret_cast<const char*>(&f.b[q]), nlen));
+  q += step(nlen);
+  int cls = -1;
+  uint32_t sz = 0;
+  bool be = false, sg = true;
+  if (!parse_dtype(f, q, tlen, &cls, &sz, &be, &sg)) return;
+  q += step(tlen) + step(slen);
+  if (f.ok(q, sz)) ds->attrs[an] = scalar_value(f, q, cls, sz, be);
+}
+
+// Data layout message, versions 3 and 4.
+void parse_layout(const File& f, uint64_t body, uint64_t len, Dataset* ds) {
+  if (len < 2 || !f.ok(body, len)) return;
+  const int ver = f.b[body];
+  ds->layout_version = ver;
+  if (ver != 3 && ver != 4) return;
+  ds->layout = f.b[body + 1];
+  if (ds->layout == 1 && len >= 18) {  // contiguous: address, size
+    ds->addr = f.get<uint64_t>(body + 2);
+    ds->nbytes = f.get<uint64_t>(body + 10);
+    return;
+  }
+  if (ds->layout != 2) return;
+  ds->chunk.clear();
+  if (ver == 3) {
+    // dimensionality (rank + 1), B-tree address, 4-byte sizes (the last
+    // one is the element size)
+    if (len < 11) return;
+    const int nd = f.b[body + 2];
+    ds->addr = f.get<uint64_t>(body + 3);
+    if (!f.ok(body + 11, uint64_t(nd) * 4)) return;
+    for (int i = 0; i + 1 < nd; i++) ds->chunk.push_back(f.get<uint32_t>(body + 11 + 4 * uint64_t(i)));
+    ds->index_type = 0;
+    return;
+  }
+  // version 4: flags, dimensionality, size of the encoded dimensions,
+  // dimensions, index type, index-specific fields, address
+  if (len < 5) return;
+  const int flags = f.b[body + 2], nd = f.b[body + 3], enc = f.b[body + 4];
+  uint64_t q = body + 5;
+  if (enc < 1 || enc > 8 || !f.ok(q, uint64_t(nd) * enc + 1)) return;
+  for (int i = 0; i < nd; i++) ds->chunk.push_back(f.getn(q + uint64_t(i) * enc, enc));
+  if (!ds->chunk.empty()) ds->chunk.pop_back();  // the element size
+  q += uint64_t(nd) * enc;
+  ds->index_type = f.b[q++];
+  if (ds->index_type == 1) {  // single chunk: [filtered size, filter mask]
+    if (flags & 2) q += 8 + 4;
+  } else if (ds->index_type == 3) {  // fixed array: page bits
+    q += 1;
+  } else if (ds->index_type == 4) {  // extensible array parameters
+    q += 5;
+  } else if (ds->index_type == 5) {  // version-2 B-tree parameters
+    q += 6;
+  }
+  if (f.ok(q, 8)) ds->addr = f.get<uint64_t>(q);
+}
+
+// The messages of an object header of version 1 or 2 (with its
+// continuation blocks): dataset fields into *ds, group fields into *grp.
+bool parse_object(const File& f, uint64_t oh, Dataset* ds, GroupInfo* grp) {
   struct Block {
     uint64_t at, len;
   };
-  std::vector<Block> blocks{{oh + 16, f.get<uint32_t>(oh + 8)}};
+  std::vector<Block> blocks;
+  int version = 0, nmsg = 1 << 30;
+  bool creation_order = false;
+  if (f.ok(oh, 16) && f.b[oh] == 1) {
+    version = 1;
+    nmsg = f.get<uint16_t>(oh + 2);
+    blocks.push_back({oh + 16, f.get<uint32_t>(oh + 8)});
+  } else if (f.ok(oh, 6) && std::memcmp(&f.b[oh], "OHDR", 4) == 0 && f.b[oh + 4] == 2) {
+    version = 2;
+    const int flags = f.b[oh + 5];
+    uint64_t q = oh + 6;
+    if (flags & 0x20) q += 16;  // access, modification, change, birth times
+    if (flags & 0x10) q += 4;   // attribute storage phase change values
+    const int sz = 1 << (flags & 3);
+    if (!f.ok(q, uint64_t(sz))) return false;
+    const uint64_t chunk0 = f.getn(q, sz);
+    q += uint64_t(sz);
+    blocks.push_back({q, chunk0});
+    creation_order = (flags & 0x04) != 0;
+  } else {
+    return false;
+  }
   int seen = 0;
   for (size_t bi = 0; bi < blocks.size() && seen < nmsg && bi < 64; bi++) {
     uint64_t p = blocks[bi].at;
     const uint64_t end = blocks[bi].at + blocks[bi].len;
-    while (p + 8 <= end && seen < nmsg) {
-      if (!f.ok(p, 8)) return false;
-      const uint16_t type = f.get<uint16_t>(p), len = f.get<uint16_t>(p + 2);
-      const uint64_t body = p + 8;
-      if (!f.ok(body, len)) return false;
+    if (!f.ok(p, blocks[bi].len)) return false;
+    const uint64_t hsize = version == 1 ? 8 : (creation_order ? 6 : 4);
+    while (p + hsize <= end && seen < nmsg) {
+      uint16_t type;
+      uint64_t len;
+      if (version == 1) {
+        type = f.get<uint16_t>(p);
+        len = f.get<uint16_t>(p + 2);
+      } else {
+        type = f.b[p];
+        len = f.get<uint16_t>(p + 1);
+      }
+      const uint64_t body = p + hsize;
+      if (!f.ok(body, len) || body + len > end) return false;
       seen++;
       switch (type) {
         case 0x0001:
           if (ds) parse_dataspace(f, body, len, &ds->dims);
           break;
+        case 0x0002:  // link info: a fractal heap address means dense links
+          if (grp && len >= 10) {
+            const int lflags = f.b[body + 1];
+            const uint64_t heap_at = body + 2 + ((lflags & 1) ? 8 : 0);
+            if (f.ok(heap_at, 8) && f.get<uint64_t>(heap_at) != kUndef) grp->dense_links = true;
+          }
+          break;
         case 0x0003:
           if (ds) parse_dtype(f, body, len, &ds->cls, &ds->size, &ds->big_endian, &ds->is_signed);
           break;
+        case 0x0006:  // link (version 1)
+          if (grp && len >= 4 && f.b[body] == 1) {
+            const int lf = f.b[body + 1];
+            uint64_t q = body + 2;
+            int ltype = 0;
+            if (lf & 0x08) ltype = f.b[q++];
+            if (lf & 0x04) q += 8;
+            if (lf & 0x10) q += 1;
+            const int nb = 1 << (lf & 3);
+            if (!f.ok(q, uint64_t(nb))) break;
+            const uint64_t nl = f.getn(q, nb);
+            q += uint64_t(nb);
+            if (ltype != 0 || !f.ok(q, nl + 8)) break;  // hard links only
+            grp->links[std::string(reinterpret_cast<const char*>(&f.b[q]), size_t(nl))] = f.get<uint64_t>(q + nl);
+          }
+          break;
         case 0x0008:
-          if (ds && len >= 2) {
-            const int ver = f.b[body];
-            if (ver == 3) {
-              ds->layout = f.b[body + 1];
-              if (ds->layout == 1 && len >= 18) {
-                ds->addr = f.get<uint64_t>(body + 2);
-                ds->nbytes = f.get<uint64_t>(body + 10);
-              }
+          if (ds) parse_layout(f, body, len, ds);
+          break;
+        case 0x000B:  // filter pipeline: compressed or otherwise filtered data
+          if (ds) ds->filtered = true;
+          break;
+        case 0x000C:
+          if (ds) parse_attribute(f, body, len, ds);
+          break;
+        case 0x0010:  // continuation
+          if (len >= 16) {
+            const uint64_t at = f.get<uint64_t>(body), l = f.get<uint64_t>(body + 8);
+            if (version == 1) {
+              blocks.push_back({at, l});
+            } else if (f.ok(at, 4) && std::memcmp(&f.b[at], "OCHK", 4) == 0 && l >= 8) {
+              blocks.push_back({at + 4, l - 8});  // signature and checksum
             }
           }
           break;
-        case 0x000C:
-          if (ds && len >= 8 && f.b[body] == 1) {
-            const uint16_t nlen = f.get<uint16_t>(body + 2), tlen = f.get<uint16_t>(body + 4),
-                           slen = f.get<uint16_t>(body + 6);
-            uint64_t q = body + 8;
-            if (!f.ok(q, nlen)) break;
-            std::string an(reinterpret_cast<const char*>(&f.b[q]), strnlen(reinterpret_cast<const char*>(&f.b[q]), nlen));
-            q += up8(nlen);
-            int cls = -1;
-            uint32_t sz = 0;
-            bool be = false, sg = true;
-            if (!parse_dtype(f, q, tlen, &cls, &sz, &be, &sg)) break;
-            q += up8(tlen) + up8(slen);
-            if (f.ok(q, sz)) ds->attrs[an] = scalar_value(f, q, cls, sz, be);
-          }
-          break;
-        case 0x0010:  // continuation
-          if (len >= 16) blocks.push_back({f.get<uint64_t>(body), f.get<uint64_t>(body + 8)});
-          break;
         case 0x0011:
-          if (btree && len >= 16) {
-            *btree = f.get<uint64_t>(body);
-            *heap = f.get<uint64_t>(body + 8);
+          if (grp && len >= 16) {
+            grp->btree = f.get<uint64_t>(body);
+            grp->heap = f.get<uint64_t>(body + 8);
           }
           break;
         default:
@@ -452,6 +596,12 @@ uint64_t find_in_group(const File& f, uint64_t btree, uint64_t heap, const std::
   return kUndef;
 }
 
+uint64_t element_count(const Dataset& ds) {
+  uint64_t count = 1;
+  for (uint64_t d : ds.dims) count *= d;
+  return count;
+}
+
 int open_dataset(const char* path, const char* name, File* f, Dataset* ds) {
   if (!path || !name) return h5_fail(RAPTR_H5_INVALID, "bad argument");
   FILE* fp = std::fopen(path, "rb");
@@ -464,32 +614,184 @@ int open_dataset(const char* path, const char* name, File* f, Dataset* ds) {
   std::fclose(fp);
   if (r != f->b.size()) return h5_fail(RAPTR_H5_IO, std::string("cannot read ") + path);
   const uint8_t sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
-  if (f->b.size() < 96 || std::memcmp(f->b.data(), sig, 8) != 0)
+  if (f->b.size() < 48 || std::memcmp(f->b.data(), sig, 8) != 0)
     return h5_fail(RAPTR_H5_FORMAT, std::string(path) + " is not an HDF5 file");
   const int sbv = f->b[8];
-  if (sbv > 1 || f->b[13] != 8 || f->b[14] != 8)
-    return h5_fail(RAPTR_H5_UNSUPPORTED, "only superblock versions 0/1 with 8-byte offsets are read");
-  // root symbol table entry follows the fixed fields (v1 has 4 more bytes)
-  const uint64_t root = 24 + (sbv == 1 ? 4 : 0) + 32;
-  const uint64_t root_oh = f->get<uint64_t>(root + 8);
-  uint64_t btree = kUndef, heap = kUndef;
-  if (f->get<uint32_t>(root + 16) == 1) {
-    btree = f->get<uint64_t>(root + 24);
-    heap = f->get<uint64_t>(root + 32);
+  GroupInfo root;
+  if (sbv <= 1) {
+    if (f->b.size() < 96 || f->b[13] != 8 || f->b[14] != 8)
+      return h5_fail(RAPTR_H5_UNSUPPORTED, "only 8-byte offsets and lengths are read");
+    // root symbol table entry follows the fixed fields (v1 has 4 more bytes)
+    const uint64_t at = 24 + (sbv == 1 ? 4 : 0) + 32;
+    const uint64_t root_oh = f->get<uint64_t>(at + 8);
+    if (f->get<uint32_t>(at + 16) == 1) {
+      root.btree = f->get<uint64_t>(at + 24);
+      root.heap = f->get<uint64_t>(at + 32);
+    }
+    if (root.btree == kUndef && !parse_object(*f, root_oh, nullptr, &root))
+      return h5_fail(RAPTR_H5_FORMAT, "cannot read the root group");
+  } else if (sbv == 2 || sbv == 3) {
+    if (f->b[9] != 8 || f->b[10] != 8) return h5_fail(RAPTR_H5_UNSUPPORTED, "only 8-byte offsets and lengths are read");
+    const uint64_t root_oh = f->get<uint64_t>(36);
+    if (!parse_object(*f, root_oh, nullptr, &root)) return h5_fail(RAPTR_H5_FORMAT, "cannot read the root group");
+  } else {
+    return h5_fail(RAPTR_H5_UNSUPPORTED, "superblock version " + std::to_string(sbv) + " is not read");
   }
-  if (btree == kUndef && !parse_object(*f, root_oh, nullptr, &btree, &heap))
-    return h5_fail(RAPTR_H5_FORMAT, "cannot read the root group");
-  const uint64_t oh = find_in_group(*f, btree, heap, name);
+  uint64_t oh = kUndef;
+  if (root.btree != kUndef) {
+    oh = find_in_group(*f, root.btree, root.heap, name);
+  } else {
+    auto it = root.links.find(name);
+    if (it != root.links.end()) oh = it->second;
+    else if (root.dense_links)
+      return h5_fail(RAPTR_H5_UNSUPPORTED, "the root group keeps its links in dense storage (a fractal heap)");
+  }
   if (oh == kUndef) return h5_fail(RAPTR_H5_NOT_FOUND, std::string("no dataset \"") + name + "\" in " + path);
-  if (!parse_object(*f, oh, ds, nullptr, nullptr)) return h5_fail(RAPTR_H5_FORMAT, "cannot read the dataset header");
-  if (ds->layout != 1 || ds->addr == kUndef)
-    return h5_fail(RAPTR_H5_UNSUPPORTED, "only contiguous datasets are read");
+  if (!parse_object(*f, oh, ds, nullptr)) return h5_fail(RAPTR_H5_FORMAT, "cannot read the dataset header");
   if (ds->big_endian || !((ds->cls == 1 && (ds->size == 4 || ds->size == 8)) || (ds->cls == 0 && ds->size == 4)))
     return h5_fail(RAPTR_H5_UNSUPPORTED, "only little-endian float32/float64/int32 datasets are read");
-  uint64_t count = 1;
-  for (uint64_t d : ds->dims) count *= d;
-  if (ds->nbytes < count * ds->size || !f->ok(ds->addr, count * ds->size))
-    return h5_fail(RAPTR_H5_FORMAT, "dataset extends past the end of the file");
+  if (ds->filtered) return h5_fail(RAPTR_H5_UNSUPPORTED, "filtered (compressed) datasets are not read");
+  const uint64_t count = element_count(*ds);
+  if (ds->layout == 1) {
+    if (ds->addr == kUndef) return h5_fail(RAPTR_H5_FORMAT, "contiguous dataset without data");
+    if (ds->nbytes < count * ds->size || !f->ok(ds->addr, count * ds->size))
+      return h5_fail(RAPTR_H5_FORMAT, "dataset extends past the end of the file");
+    return RAPTR_H5_OK;
+  }
+  if (ds->layout == 2) {
+    if (ds->chunk.size() != ds->dims.size() || ds->addr == kUndef)
+      return h5_fail(RAPTR_H5_FORMAT, "chunked dataset without its chunk dimensions or index");
+    for (uint64_t c : ds->chunk)
+      if (c == 0) return h5_fail(RAPTR_H5_FORMAT, "zero chunk dimension");
+    if (ds->layout_version == 4 && !(ds->index_type >= 1 && ds->index_type <= 3))
+      return h5_fail(RAPTR_H5_UNSUPPORTED, "chunk index type " + std::to_string(ds->index_type) +
+                                               " (extensible array or version-2 B-tree) is not read");
+    return RAPTR_H5_OK;
+  }
+  return h5_fail(RAPTR_H5_UNSUPPORTED, "only contiguous and chunked datasets are read");
+}
+
+float element_at(const File& f, const Dataset& ds, uint64_t at) {
+  return ds.cls == 1 ? (ds.size == 4 ? f.get<float>(at) : float(f.get<double>(at))) : float(f.get<int32_t>(at));
+}
+
+// Copies one chunk (dense, chunk dims, at file offset `at`) whose first
+// element sits at dataset coordinates `org` into out (row-major dataset),
+// clipping at the dataset's edges.
+bool copy_chunk(const File& f, const Dataset& ds, uint64_t at, const std::vector<uint64_t>& org, float* out) {
+  const size_t r = ds.dims.size();
+  uint64_t celems = 1;
+  for (uint64_t c : ds.chunk) celems *= c;
+  if (!f.ok(at, celems * ds.size)) return false;
+  for (size_t d = 0; d < r; d++)
+    if (org[d] >= ds.dims[d]) return false;
+  std::vector<uint64_t> idx(r, 0);
+  for (uint64_t e = 0; e < celems; e++) {
+    // element e of the chunk, row-major: idx
+    uint64_t rem = e, flat = 0;
+    bool inside = true;
+    for (size_t d = r; d-- > 0;) {
+      idx[d] = rem % ds.chunk[d];
+      rem /= ds.chunk[d];
+    }
+    for (size_t d = 0; d < r; d++) {
+      const uint64_t c = org[d] + idx[d];
+      if (c >= ds.dims[d]) {
+        inside = false;
+        break;
+      }
+      flat = flat * ds.dims[d] + c;
+    }
+    if (inside) out[flat] = element_at(f, ds, at + e * ds.size);
+  }
+  return true;
+}
+
+// Chunks of a version-1 B-tree (node type 1) below `node`.
+bool read_btree_chunks(const File& f, const Dataset& ds, uint64_t node, float* out, int depth, uint64_t* nchunks) {
+  if (depth > 64 || !f.ok(node, 24) || std::memcmp(&f.b[node], "TREE", 4) != 0 || f.b[node + 4] != 1) return false;
+  const int level = f.b[node + 5], used = f.get<uint16_t>(node + 6);
+  const size_t r = ds.dims.size();
+  const uint64_t key = 8 + 8 * (r + 1);  // chunk size, filter mask, r + 1 offsets
+  uint64_t p = node + 24;
+  for (int i = 0; i < used; i++) {
+    if (!f.ok(p, key + 8)) return false;
+    const uint32_t mask = f.get<uint32_t>(p + 4);
+    std::vector<uint64_t> org(r);
+    for (size_t d = 0; d < r; d++) org[d] = f.get<uint64_t>(p + 8 + 8 * d);
+    const uint64_t child = f.get<uint64_t>(p + key);
+    if (level > 0) {
+      if (!read_btree_chunks(f, ds, child, out, depth + 1, nchunks)) return false;
+    } else {
+      if (mask != 0) return false;
+      if (!copy_chunk(f, ds, child, org, out)) return false;
+      ++*nchunks;
+    }
+    p += key + 8;
+  }
+  return true;
+}
+
+// Reads every element of the dataset into out (row-major, count elements).
+int read_elements(const File& f, const Dataset& ds, float* out) {
+  const uint64_t count = element_count(ds);
+  if (ds.layout == 1) {
+    for (uint64_t i = 0; i < count; i++) out[i] = element_at(f, ds, ds.addr + i * ds.size);
+    return RAPTR_H5_OK;
+  }
+  // chunked: elements no chunk covers keep the fill value 0
+  std::fill(out, out + count, 0.f);
+  const size_t r = ds.dims.size();
+  std::vector<uint64_t> grid(r);  // chunks per dimension
+  uint64_t nchunk_all = 1;
+  for (size_t d = 0; d < r; d++) {
+    grid[d] = (ds.dims[d] + ds.chunk[d] - 1) / ds.chunk[d];
+    nchunk_all *= grid[d];
+  }
+  uint64_t celems = 1;
+  for (uint64_t c : ds.chunk) celems *= c;
+  auto origin = [&](uint64_t k) {  // chunk k in row-major chunk order
+    std::vector<uint64_t> org(r);
+    for (size_t d = r; d-- > 0;) {
+      org[d] = (k % grid[d]) * ds.chunk[d];
+      k /= grid[d];
+    }
+    return org;
+  };
+  if (ds.layout_version == 3) {
+    uint64_t n = 0;
+    if (!read_btree_chunks(f, ds, ds.addr, out, 0, &n))
+      return h5_fail(RAPTR_H5_FORMAT, "damaged or filtered chunk B-tree");
+    return RAPTR_H5_OK;
+  }
+  if (ds.index_type == 1) {  // one chunk holds the whole dataset
+    if (!copy_chunk(f, ds, ds.addr, std::vector<uint64_t>(r, 0), out))
+      return h5_fail(RAPTR_H5_FORMAT, "single chunk extends past the end of the file");
+    return RAPTR_H5_OK;
+  }
+  if (ds.index_type == 2) {  // implicit: every chunk, in chunk order, back to back
+    for (uint64_t k = 0; k < nchunk_all; k++)
+      if (!copy_chunk(f, ds, ds.addr + k * celems * ds.size, origin(k), out))
+        return h5_fail(RAPTR_H5_FORMAT, "implicit chunks extend past the end of the file");
+    return RAPTR_H5_OK;
+  }
+  // fixed array: header "FAHD" -> data block "FADB" of chunk addresses
+  const uint64_t h = ds.addr;
+  if (!f.ok(h, 28) || std::memcmp(&f.b[h], "FAHD", 4) != 0)
+    return h5_fail(RAPTR_H5_FORMAT, "fixed-array chunk index without its header");
+  const int client = f.b[h + 5], esize = f.b[h + 6], page_bits = f.b[h + 7];
+  const uint64_t nelem = f.get<uint64_t>(h + 8), block = f.get<uint64_t>(h + 16);
+  if (client != 0 || esize != 8) return h5_fail(RAPTR_H5_UNSUPPORTED, "filtered fixed-array chunk index");
+  if (page_bits < 64 && nelem > (uint64_t(1) << page_bits))
+    return h5_fail(RAPTR_H5_UNSUPPORTED, "paged fixed-array chunk index");
+  if (nelem != nchunk_all || !f.ok(block, 14 + nelem * 8) || std::memcmp(&f.b[block], "FADB", 4) != 0)
+    return h5_fail(RAPTR_H5_FORMAT, "fixed-array chunk index does not match the dataset");
+  for (uint64_t k = 0; k < nelem; k++) {
+    const uint64_t at = f.get<uint64_t>(block + 14 + k * 8);
+    if (at == kUndef) continue;  // never written: fill value
+    if (!copy_chunk(f, ds, at, origin(k), out))
+      return h5_fail(RAPTR_H5_FORMAT, "chunk extends past the end of the file");
+  }
   return RAPTR_H5_OK;
 }
 
@@ -543,11 +845,7 @@ int raptr_h5_read_f32(const char* path, const char* name, float* out, int64_t ca
   if (count) *count = int64_t(n);
   if (!out) return RAPTR_H5_OK;
   if (int64_t(n) > capacity) return h5_fail(RAPTR_H5_INVALID, "buffer too small");
-  for (uint64_t i = 0; i < n; i++) {
-    const uint64_t at = ds.addr + i * ds.size;
-    out[i] = ds.cls == 1 ? (ds.size == 4 ? f.get<float>(at) : float(f.get<double>(at))) : float(f.get<int32_t>(at));
-  }
-  return RAPTR_H5_OK;
+  return read_elements(f, ds, out);
 }
 
 int raptr_h5_read_density_grid(const char* path, int32_t n[3], float lo[3], float hi[3]) {
