@@ -7,8 +7,11 @@
 // sizes.  Blocks of at least kMinCached bytes are therefore not returned
 // to the driver when the library frees them but parked per device, and a
 // later request of a similar size (up to 25 % smaller) takes the smallest
-// fitting parked block.  Parked bytes per device are capped at half the
-// device's memory; when an allocation fails, the device's parked blocks
+// fitting parked block.  Parked bytes per device are capped at two thirds
+// of the device's memory, which holds every block of a full reconstruction
+// job (matrix, transpose and the transpose's staging, ~107 GB at 70^3 x
+// 5.14M channels), so that the next job of the same size allocates nothing
+// from the driver; when an allocation fails, the device's parked blocks
 // are released and the allocation is retried once.  raptr_trim_memory()
 // releases them on request (before a caller allocates much memory by other
 // means, say).
@@ -116,7 +119,7 @@ void dev_free(void* p) {
     }
     if (ok) {
       total = g_total[b.device];
-      park = g_parked_bytes[b.device] + b.bytes <= total / 2;
+      park = g_parked_bytes[b.device] + b.bytes <= total / 3 * 2;
       if (park) {
         g_parked[b.device].emplace(b.bytes, p);
         g_parked_bytes[b.device] += b.bytes;

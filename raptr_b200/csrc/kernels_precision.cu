@@ -158,56 +158,7 @@ __device__ __forceinline__ float row_dot_half(const int32_t* __restrict__ col, c
   return warp_sum_f((acc0 + acc1) + (acc2 + acc3));
 }
 
-// Row dot with binary16 values in quads: after a head of up to 3 entries
-// (which brings the index to a multiple of 4), lane q takes quads q, q+32,
-// ... (four consecutive entries: one 16-byte index load and one 8-byte
-// value load), four quads per lane in flight, then up to 3 tail entries.
-// Needs col 16-byte and hv 8-byte aligned.
-__device__ __forceinline__ float row_dot_half_quads(const int32_t* __restrict__ col, const uint16_t* __restrict__ hv,
-                                                    int64_t b, int64_t e, const float* __restrict__ x, int lane) {
-  float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
-  int64_t a = (b + 3) & ~int64_t(3);
-  if (a > e) a = e;
-  if (b + lane < a) acc0 += h2f(__ldcs(reinterpret_cast<const unsigned short*>(hv) + b + lane)) *
-                            __ldg(x + __ldcs(col + b + lane));
-  const int64_t nq = (e - a) >> 2;
-  const int4* c4 = reinterpret_cast<const int4*>(col + a);
-  const uint2* h4 = reinterpret_cast<const uint2*>(hv + a);
-  int64_t q = lane;
-  for (; q + 96 < nq; q += 128) {
-    const int4 c0 = __ldcs(c4 + q), c1 = __ldcs(c4 + q + 32), c2 = __ldcs(c4 + q + 64), c3 = __ldcs(c4 + q + 96);
-    const uint2 w0 = __ldcs(h4 + q), w1 = __ldcs(h4 + q + 32), w2 = __ldcs(h4 + q + 64), w3 = __ldcs(h4 + q + 96);
-    const float g00 = __ldg(x + c0.x), g01 = __ldg(x + c0.y), g02 = __ldg(x + c0.z), g03 = __ldg(x + c0.w);
-    const float g10 = __ldg(x + c1.x), g11 = __ldg(x + c1.y), g12 = __ldg(x + c1.z), g13 = __ldg(x + c1.w);
-    const float g20 = __ldg(x + c2.x), g21 = __ldg(x + c2.y), g22 = __ldg(x + c2.z), g23 = __ldg(x + c2.w);
-    const float g30 = __ldg(x + c3.x), g31 = __ldg(x + c3.y), g32 = __ldg(x + c3.z), g33 = __ldg(x + c3.w);
-    const float2 f00 = __half22float2(*reinterpret_cast<const __half2*>(&w0.x));
-    const float2 f01 = __half22float2(*reinterpret_cast<const __half2*>(&w0.y));
-    const float2 f10 = __half22float2(*reinterpret_cast<const __half2*>(&w1.x));
-    const float2 f11 = __half22float2(*reinterpret_cast<const __half2*>(&w1.y));
-    const float2 f20 = __half22float2(*reinterpret_cast<const __half2*>(&w2.x));
-    const float2 f21 = __half22float2(*reinterpret_cast<const __half2*>(&w2.y));
-    const float2 f30 = __half22float2(*reinterpret_cast<const __half2*>(&w3.x));
-    const float2 f31 = __half22float2(*reinterpret_cast<const __half2*>(&w3.y));
-    acc0 += f00.x * g00 + f00.y * g01 + f01.x * g02 + f01.y * g03;
-    acc1 += f10.x * g10 + f10.y * g11 + f11.x * g12 + f11.y * g13;
-    acc2 += f20.x * g20 + f20.y * g21 + f21.x * g22 + f21.y * g23;
-    acc3 += f30.x * g30 + f30.y * g31 + f31.x * g32 + f31.y * g33;
-  }
-  for (; q < nq; q += 32) {
-    const int4 c0 = __ldcs(c4 + q);
-    const uint2 w0 = __ldcs(h4 + q);
-    const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&w0.x));
-    const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&w0.y));
-    acc1 += f0.x * __ldg(x + c0.x) + f0.y * __ldg(x + c0.y) + f1.x * __ldg(x + c0.z) + f1.y * __ldg(x + c0.w);
-  }
-  const int64_t t = a + (nq << 2) + lane;
-  if (t < e) acc2 += h2f(__ldcs(reinterpret_cast<const unsigned short*>(hv) + t)) * __ldg(x + __ldcs(col + t));
-  return warp_sum_f((acc0 + acc1) + (acc2 + acc3));
-}
-
 // e'[rank_i] = scale_i * y_i / (A x)_i, 0 where y_i == 0.
-template <bool QUADS>
 __global__ void __launch_bounds__(kThreads) mlem_forward_half_kernel(
     int64_t m, const int64_t* __restrict__ rp, const int32_t* __restrict__ col, const uint16_t* __restrict__ hval,
     const float* __restrict__ rscale, const float* __restrict__ y, const float* __restrict__ x,
@@ -223,8 +174,7 @@ __global__ void __launch_bounds__(kThreads) mlem_forward_half_kernel(
       continue;
     }
     const float sc = __ldg(rscale + r);
-    const float yt = sc * (QUADS ? row_dot_half_quads(col, hval, rp[r], rp[r + 1], x, lane)
-                                 : row_dot_half(col, hval, rp[r], rp[r + 1], x, lane));
+    const float yt = sc * row_dot_half(col, hval, rp[r], rp[r + 1], x, lane);
     if (lane == 0) {
       e[dst] = sc * __fdiv_rn(yi, yt);
       if (ll) {
@@ -425,10 +375,7 @@ cudaError_t launch_mlem_forward_half(int64_t m, const int64_t* rp, const int32_t
                                      const float* rscale, const float* y, const float* x, const int32_t* rank,
                                      float* e, double* d_ll, cudaStream_t s) {
   if (m <= 0) return cudaSuccess;
-  if ((reinterpret_cast<uintptr_t>(col) & 15) == 0 && (reinterpret_cast<uintptr_t>(hval) & 7) == 0)
-    mlem_forward_half_kernel<true><<<grid_rows(m), kThreads, 0, s>>>(m, rp, col, hval, rscale, y, x, rank, e, d_ll);
-  else
-    mlem_forward_half_kernel<false><<<grid_rows(m), kThreads, 0, s>>>(m, rp, col, hval, rscale, y, x, rank, e, d_ll);
+  mlem_forward_half_kernel<<<grid_rows(m), kThreads, 0, s>>>(m, rp, col, hval, rscale, y, x, rank, e, d_ll);
   note_launches(1);
   return cudaGetLastError();
 }
