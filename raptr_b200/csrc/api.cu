@@ -143,6 +143,14 @@ raptr_status set_error(raptr_status st, const std::string& msg) { return fail(st
 // Context and matrix objects
 // ---------------------------------------------------------------------------
 
+namespace raptr {
+// The batched back pass in row-block groups (BatchArgs.seg): blocks of the
+// transpose's row order, and the ratio bytes of one frame tile above which
+// the grouping is used.
+constexpr int kBatchRowBlocks = 16;
+constexpr double kBatchBlockingBytes = 96.0 * (1 << 20);
+}  // namespace raptr
+
 struct raptr_ctx {
   raptr_geom geom;
   DGeom dg;
@@ -161,6 +169,27 @@ struct raptr_ctx {
   // Voxels in compact (y, z) tubes along x: the column order of the
   // batched back pass, built on first use.
   int32_t* d_col_order = nullptr;
+  // Row-block offsets of the columns of a transpose (see BatchArgs.seg),
+  // computed for every batched call (a transpose's arrays can be freed and
+  // their memory reused by another, so nothing is cached by address).
+  int32_t* d_bseg = nullptr;
+  int64_t bseg_n = -1;
+
+  cudaError_t block_seg(const int64_t* cp, const int32_t* trow, int64_t m, int64_t n, cudaStream_t s,
+                        const int32_t** out) {
+    if (bseg_n < n) {
+      dev_free(d_bseg);
+      d_bseg = nullptr;
+      bseg_n = -1;
+      cudaError_t e = dev_malloc(&d_bseg, size_t(n) * (kBatchRowBlocks + 1) * sizeof(int32_t));
+      if (e != cudaSuccess) return e;
+      bseg_n = n;
+    }
+    cudaError_t e = launch_block_seg(n, m, kBatchRowBlocks, cp, trow, d_bseg, s);
+    if (e != cudaSuccess) return e;
+    *out = d_bseg;
+    return cudaSuccess;
+  }
 
   cudaError_t col_order(const int32_t** out) {
     if (!d_col_order) {
@@ -582,6 +611,7 @@ raptr_status raptr_ctx_destroy(raptr_ctx* ctx) {
   dev_free(ctx->d_flags);
   dev_free(ctx->d_f64);
   dev_free(ctx->d_col_order);
+  dev_free(ctx->d_bseg);
   cudaFreeHost(ctx->h_pin);
   delete ctx;
   return RAPTR_OK;
@@ -1447,7 +1477,8 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
   const bool use_graph = opts && opts->use_graph && !want_times;
   RCHECK(ctx->ensure_scratch(Carve::need({size_t(std::max<int64_t>(m, 1)) * n_frames * sizeof(float),
                                           size_t(n) * n_frames * sizeof(float), size_t(n_frames) * sizeof(double),
-                                          size_t(n_frames) * sizeof(unsigned long long)})));
+                                          size_t(n_frames) * sizeof(unsigned long long) * kBatchRowBlocks,
+                                          size_t(n) * std::min(kt, int(n_frames)) * sizeof(float)})));
   Carve cv(ctx->d_scratch);
   // the tube order of the back pass applies when the columns are the
   // context's voxels
@@ -1455,7 +1486,13 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
   a.E = cv.take<float>(size_t(std::max<int64_t>(m, 1)) * n_frames);
   a.XX = cv.take<float>(size_t(n) * n_frames);
   double* acc = cv.take<double>(size_t(n_frames));
-  unsigned long long* next = cv.take<unsigned long long>(size_t(n_frames));
+  unsigned long long* next = cv.take<unsigned long long>(size_t(n_frames) * kBatchRowBlocks);
+  // the back pass in row-block groups when one tile's ratios exceed L2
+  if (m > 0 && double(m) * std::min(kt, int(n_frames)) * sizeof(float) > kBatchBlockingBytes) {
+    RCU(ctx->block_seg(d_col_ptr, d_row_idx, m, n, s, &a.seg));
+    a.seg_blocks = kBatchRowBlocks;
+    a.P = cv.take<float>(size_t(n) * std::min(kt, int(n_frames)));
+  }
   std::vector<cudaEvent_t> evs;
   if (want_times) {
     evs.resize(size_t(3 * n_iter));

@@ -182,15 +182,25 @@ struct BatchArgs {
   float* X = nullptr;
   float* E = nullptr;
   float* XX = nullptr;
+  // Row blocks of the transpose's order for the back pass (may be null):
+  // seg (n x (seg_blocks+1) int32, launch_block_seg) and the partial sums P
+  // (n x the largest tile floats).
+  const int32_t* seg = nullptr;
+  int seg_blocks = 0;
+  float* P = nullptr;
 };
+// The row-block offsets of every column of a transpose (see BatchArgs.seg):
+// seg[j*(B+1) + b] = offset in column j of its first entry with row >= b*m/B.
+cudaError_t launch_block_seg(int64_t n, int64_t m, int B, const int64_t* cp, const int32_t* trow, int32_t* seg,
+                             cudaStream_t s);
 // K frames (a multiple of 4) in tiles of at most kt (4, 8, 16, 32 or 64).
 bool batch_tile_supported(int K, int kt);
 // The tile that starts at frame f0: kt while kt frames remain, else the
 // largest power of two that fits.
 int batch_tile_at(int K, int kt, int f0);
 // One iteration for all K frames in tiles of at most kt frames (acc: K
-// doubles, next: K/4 work counters, both scratch); ev_mid, when set, is
-// recorded between the two passes.
+// doubles, next: K/4 * max(1, seg_blocks) work counters, both scratch);
+// ev_mid, when set, is recorded between the two passes.
 cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, unsigned long long* next, cudaStream_t s,
                                    cudaEvent_t ev_mid);
 

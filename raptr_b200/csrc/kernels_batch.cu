@@ -14,7 +14,9 @@
 // back pass can take the columns in a given order: voxels in compact
 // (y, z) tubes along x keep the ratio rows that concurrent warps gather
 // (the channels crossing those voxels) within L2.
+#include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include <cuda_fp16.h>
 
@@ -37,6 +39,7 @@ unsigned grid_warps(int64_t items) {
 }
 
 constexpr int kColsPerWarp = 48;  // back pass: columns a warp takes before its block ends
+constexpr double kBackGroupBytes = 48.0 * (1 << 20);  // ratios of a back-pass row-block group
 
 __device__ __forceinline__ float to_f(float v) { return v; }
 __device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
@@ -111,6 +114,14 @@ __global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int 
 // c = sum_k v_kj E[k*K + f] (FP32; the FP16 values dominate its error),
 // XX = X*c/(S+(S==0)), acc[f] += sum_j XX (FP64).  Warps take columns from
 // the counter *next (zero at launch).
+//
+// With a row-block group (seg non-null), only the column's entries whose
+// rows lie in blocks [b0, b1) of the transpose's row order are summed
+// (entries seg[j*segw + b0] .. seg[j*segw + b1] of column j): the ratios of
+// those rows then stay in L2 while every column reads them.  The partial
+// sums of all but the last group go to P (n x KT, tile-local frames); the
+// last group adds them and finishes as above.  mode: 0 = the whole column
+// at once, 1 = first group, 2 = a middle group, 3 = the last group.
 template <int KT, typename VT>
 __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, int f0, unsigned long long* next,
                                                               const int64_t* __restrict__ cp,
@@ -120,7 +131,9 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
                                                               const float* __restrict__ X,
                                                               const float* __restrict__ sens,
                                                               const int32_t* __restrict__ col_order,
-                                                              float* __restrict__ XX, double* __restrict__ acc) {
+                                                              float* __restrict__ XX, double* __restrict__ acc,
+                                                              const int32_t* __restrict__ seg, int segw, int b0,
+                                                              int b1, int mode, float* __restrict__ P) {
   using S = Split<KT>;
   const int lane = threadIdx.x & 31;
   const int es = lane / S::LPE, fg = lane % S::LPE;
@@ -143,7 +156,12 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
     float s[S::VEC];
 #pragma unroll
     for (int v = 0; v < S::VEC; v++) s[v] = 0.f;
-    const int64_t b = cp[j], e = cp[j + 1];
+    int64_t b = cp[j], e = cp[j + 1];
+    if (seg) {
+      const int64_t c0 = b;
+      b = c0 + __ldg(seg + j * segw + b0);
+      e = c0 + __ldg(seg + j * segw + b1);
+    }
     int64_t p = b + es;
     for (; p + S::EPW < e; p += 2 * S::EPW) {
       const int k0 = __ldg(trow + p), k1 = __ldg(trow + p + S::EPW);
@@ -158,6 +176,20 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
     for (int o = S::LPE; o < 32; o <<= 1)
 #pragma unroll
       for (int v = 0; v < S::VEC; v++) s[v] += __shfl_xor_sync(0xffffffffu, s[v], o);
+    if (es == 0 && mode != 0) {
+      float4* pp = reinterpret_cast<float4*>(P + j * KT + (fbase - f0));
+      if (mode == 2 || mode == 3) {
+        const float4 q4 = *pp;
+        s[0] += q4.x;
+        s[1] += q4.y;
+        s[2] += q4.z;
+        s[3] += q4.w;
+      }
+      if (mode != 3) {
+        *pp = make_float4(s[0], s[1], s[2], s[3]);
+        continue;
+      }
+    }
     if (es == 0) {
       float dvs = __ldg(sens + j);
       dvs += float(dvs == 0.f);
@@ -188,49 +220,71 @@ __global__ void batch_normalise_kernel(int64_t n, int K, float* __restrict__ X, 
   }
 }
 
+// A back pass over row blocks [b0, b1) of the transpose (mode as in
+// batch_back_kernel; mode 0 = every row at once, without seg).
+struct BackGroup {
+  int b0 = 0, b1 = 0, mode = 0;
+};
+
 template <int KT, typename VT>
-cudaError_t launch_tile(bool forward, int64_t m, int64_t n, int K, int f0, const int64_t* rp, const int32_t* col,
-                        const void* val, const float* rscale, const int64_t* cp, const int32_t* trow,
-                        const void* tval, const int32_t* rank, const int32_t* col_order, const float* Y,
-                        const float* S, float* X, float* E, float* XX, double* acc, unsigned long long* next,
-                        cudaStream_t s) {
+cudaError_t launch_tile(const BatchArgs& a, bool forward, int f0, double* acc, unsigned long long* next,
+                        const BackGroup& grp, cudaStream_t s) {
   if (forward)
-    batch_forward_kernel<KT, VT><<<grid_warps(m), kThreads, 0, s>>>(m, K, f0, rp, col, static_cast<const VT*>(val),
-                                                                    rscale, Y, X, rank, E);
+    batch_forward_kernel<KT, VT><<<grid_warps(a.m), kThreads, 0, s>>>(
+        a.m, a.K, f0, a.rp, a.col, static_cast<const VT*>(a.val), a.half ? a.rscale : nullptr, a.Y, a.X, a.rank, a.E);
   else
-    batch_back_kernel<KT, VT><<<unsigned((n + kColsPerWarp * (kThreads / 32) - 1) / (kColsPerWarp * (kThreads / 32))),
-                                kThreads, 0, s>>>(n, K, f0, next, cp, trow, static_cast<const VT*>(tval),
-                                                                 E, X, S, col_order, XX, acc);
+    batch_back_kernel<KT, VT><<<unsigned((a.n + kColsPerWarp * (kThreads / 32) - 1) / (kColsPerWarp * (kThreads / 32))),
+                                kThreads, 0, s>>>(a.n, a.K, f0, next, a.cp, a.trow, static_cast<const VT*>(a.tval), a.E,
+                                                  a.X, a.S, a.col_order, a.XX, acc, grp.mode ? a.seg : nullptr,
+                                                  a.seg_blocks + 1, grp.b0, grp.b1, grp.mode, a.P);
   note_launches(1);
   return cudaGetLastError();
 }
 
 template <typename VT>
-cudaError_t launch_tile_kt(int kt, bool forward, int64_t m, int64_t n, int K, int f0, const int64_t* rp,
-                           const int32_t* col, const void* val, const float* rscale, const int64_t* cp,
-                           const int32_t* trow, const void* tval, const int32_t* rank, const int32_t* col_order,
-                           const float* Y, const float* S, float* X, float* E, float* XX, double* acc,
-                           unsigned long long* next, cudaStream_t s) {
+cudaError_t launch_tile_kt(int kt, const BatchArgs& a, bool forward, int f0, double* acc, unsigned long long* next,
+                           const BackGroup& grp, cudaStream_t s) {
   switch (kt) {
-    case 4:
-      return launch_tile<4, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E, XX, acc, next, s);
-    case 8:
-      return launch_tile<8, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E, XX, acc, next, s);
-    case 16:
-      return launch_tile<16, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E,
-                                 XX, acc, next, s);
-    case 32:
-      return launch_tile<32, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E,
-                                 XX, acc, next, s);
-    case 64:
-      return launch_tile<64, VT>(forward, m, n, K, f0, rp, col, val, rscale, cp, trow, tval, rank, col_order, Y, S, X, E,
-                                 XX, acc, next, s);
-    default:
-      return cudaErrorInvalidValue;
+    case 4: return launch_tile<4, VT>(a, forward, f0, acc, next, grp, s);
+    case 8: return launch_tile<8, VT>(a, forward, f0, acc, next, grp, s);
+    case 16: return launch_tile<16, VT>(a, forward, f0, acc, next, grp, s);
+    case 32: return launch_tile<32, VT>(a, forward, f0, acc, next, grp, s);
+    case 64: return launch_tile<64, VT>(a, forward, f0, acc, next, grp, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// seg[j*(B+1) + b] = the offset in column j of its first entry whose row
+// (position in the transpose's order) is at least b*m/B: lane b of the
+// column's warp searches boundary b (entries ascend within a column).
+__global__ void block_seg_kernel(int64_t n, int64_t m, int B, const int64_t* __restrict__ cp,
+                                 const int32_t* __restrict__ trow, int32_t* __restrict__ seg) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t j = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; j < n; j += nw) {
+    const int64_t c0 = cp[j], c1 = cp[j + 1];
+    for (int b = lane; b <= B; b += 32) {
+      const int64_t kb = m * b / B;
+      int64_t lo = c0, hi = c1;  // first entry with trow >= kb
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (int64_t(__ldg(trow + mid)) < kb) lo = mid + 1;
+        else hi = mid;
+      }
+      seg[j * (B + 1) + b] = int32_t(lo - c0);
+    }
   }
 }
 
 }  // namespace
+
+cudaError_t launch_block_seg(int64_t n, int64_t m, int B, const int64_t* cp, const int32_t* trow, int32_t* seg,
+                             cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  block_seg_kernel<<<grid_warps(n), kThreads, 0, s>>>(n, m, B, cp, trow, seg);
+  note_launches(1);
+  return cudaGetLastError();
+}
 
 bool batch_tile_supported(int K, int kt) {
   return (kt == 4 || kt == 8 || kt == 16 || kt == 32 || kt == 64) && K > 0 && K % 4 == 0;
@@ -247,22 +301,50 @@ cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, unsi
   // Tiles of kt frames while that many remain, then the largest power of
   // two (>= 4, since K is a multiple of 4) that fits: 40 frames at kt = 32
   // run as 32 + 8, so no frame slot is computed for nothing.
+  // Back-pass row-block groups of a tile: the tile's ratios of one group
+  // (rows of g blocks of the transpose's order) should fit in about half of
+  // L2, so that the column gathers of the group find them there.
+  auto groups = [&](int t) {
+    std::vector<BackGroup> out;
+    if (!a.seg || !a.P || a.seg_blocks < 2) {
+      out.push_back(BackGroup{});
+      return out;
+    }
+    const double block_bytes = double(a.m) / a.seg_blocks * t * sizeof(float);
+    const int g = std::max(1, int(kBackGroupBytes / std::max(block_bytes, 1.0)));
+    if (g >= a.seg_blocks) {
+      out.push_back(BackGroup{});
+      return out;
+    }
+    for (int b = 0; b < a.seg_blocks; b += g) {
+      BackGroup q;
+      q.b0 = b;
+      q.b1 = std::min(a.seg_blocks, b + g);
+      q.mode = b == 0 ? 1 : (q.b1 == a.seg_blocks ? 3 : 2);
+      out.push_back(q);
+    }
+    return out;
+  };
+  const int ngroups_max = a.seg_blocks > 0 ? a.seg_blocks : 1;
   cudaError_t e = cudaMemsetAsync(acc, 0, size_t(a.K) * sizeof(double), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(next, 0, size_t(a.K / 4) * sizeof(unsigned long long), s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(next, 0, size_t(a.K / 4) * size_t(ngroups_max) * sizeof(unsigned long long), s);
+  const BackGroup whole;
   for (int f0 = 0; f0 < a.K && e == cudaSuccess; f0 += batch_tile_at(a.K, kt, f0)) {
     const int t = batch_tile_at(a.K, kt, f0);
-    e = a.half ? launch_tile_kt<__half>(t, true, a.m, a.n, a.K, f0, a.rp, a.col, a.val, a.rscale, a.cp, a.trow,
-                                        a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, nullptr, s)
-               : launch_tile_kt<float>(t, true, a.m, a.n, a.K, f0, a.rp, a.col, a.val, nullptr, a.cp, a.trow,
-                                       a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, nullptr, s);
+    e = a.half ? launch_tile_kt<__half>(t, a, true, f0, acc, nullptr, whole, s)
+               : launch_tile_kt<float>(t, a, true, f0, acc, nullptr, whole, s);
   }
   if (e == cudaSuccess && ev_mid) e = cudaEventRecord(ev_mid, s);
-  for (int f0 = 0, tile = 0; f0 < a.K && e == cudaSuccess; f0 += batch_tile_at(a.K, kt, f0), tile++) {
+  int counter = 0;
+  for (int f0 = 0; f0 < a.K && e == cudaSuccess; f0 += batch_tile_at(a.K, kt, f0)) {
     const int t = batch_tile_at(a.K, kt, f0);
-    e = a.half ? launch_tile_kt<__half>(t, false, a.m, a.n, a.K, f0, a.rp, a.col, a.val, a.rscale, a.cp, a.trow,
-                                        a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, next + tile, s)
-               : launch_tile_kt<float>(t, false, a.m, a.n, a.K, f0, a.rp, a.col, a.val, nullptr, a.cp, a.trow,
-                                       a.tval, a.rank, a.col_order, a.Y, a.S, a.X, a.E, a.XX, acc, next + tile, s);
+    for (const BackGroup& q : groups(t)) {
+      if (e != cudaSuccess) break;
+      e = a.half ? launch_tile_kt<__half>(t, a, false, f0, acc, next + counter, q, s)
+                 : launch_tile_kt<float>(t, a, false, f0, acc, next + counter, q, s);
+      counter++;
+    }
   }
   if (e == cudaSuccess) {
     const int64_t total = a.n * a.K;
