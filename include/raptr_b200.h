@@ -329,12 +329,18 @@ raptr_status raptr_mlem_f64(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t*
  * d_s is the one normalised sensitivity; each frame's image is normalised
  * to sum 1 after every iteration.  The matrix is FP32 (value_type 0: d_val /
  * d_tval float) or the FP16 form (value_type 1: d_val = hval, d_tval =
- * htval, d_rscale the row scales); the transpose is required and d_row_rank
- * follows it (raptr_matrix_row_order, may be null for the natural order).
+ * htval, d_rscale the row scales); value_type 2 is the FP16 form with the
+ * images and ratios gathered as bfloat16 (half the gathered bytes; each
+ * frame's image stays within 1e-3 of the FP64 iteration, and depends on no
+ * other frame).  The transpose is required and d_row_rank follows it
+ * (raptr_matrix_row_order, may be null for the natural order).  When one
+ * frame tile's ratios exceed ~96 MB, the back pass runs over groups of row
+ * blocks of the transpose so that the ratios it gathers stay in L2.
  * n_frames must be a multiple of 4.  Each pass handles up to frame_tile
  * frames per sweep of the matrix (4, 8, 16, 32 or 64; 0 = 32): tiles of
  * frame_tile frames while that many remain, then the largest power of two
- * that fits (40 frames at 32: 32 + 8).  d_x must be 16-byte aligned.
+ * that fits (40 frames at 32: 32 + 8).  d_x and d_y must be 16-byte
+ * aligned.
  * opts: use_graph captures the n_iter iterations in a CUDA graph;
  * h_kernel_ms receives per iteration the forward and back-pass times. */
 raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_frames, int32_t value_type,
@@ -422,6 +428,9 @@ typedef struct raptr_server_opts {
                                a build's transient memory (~24 bytes/entry)   */
   int32_t max_frames;       /* requests per geometry batch, 1..64              */
   int32_t keep_fp32;        /* keep the FP32 values of cached matrices         */
+  int32_t gathers;          /* 0: batches gather FP32 images and ratios
+                               (raptr_mlem_batch value_type 1); 1: bfloat16
+                               (value_type 2, half the gathered bytes)        */
 } raptr_server_opts;
 typedef struct raptr_request_stats {
   double queue_ms;   /* submit -> admitted                                    */

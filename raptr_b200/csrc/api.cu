@@ -401,7 +401,7 @@ struct Builder {
         if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_flags + b, 0, sizeof(int32_t), s);
         if (e == cudaSuccess)
           e = launch_sm_rows(level, ctx->dg, ctx->d_sincos, d_cnl, r, k, nrays, seed, d_rays, st_col[b], st_val[b],
-                             row_nnz[b], ctx->d_flags + b, s);
+                             row_nnz[b], ctx->d_flags + b, s, ctx->d_flags + 4);
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(const_cast<int32_t*>(h_flags) + b, ctx->d_flags + b, sizeof(int32_t),
                               cudaMemcpyDeviceToHost, s);
@@ -495,7 +495,7 @@ struct Builder {
       const double t0 = trace_on() ? trace_ms() : 0.0;
       RCU(cudaMemsetAsync(ctx->d_flags, 0, sizeof(int32_t), s));
       RCU(launch_sm_rows(level, ctx->dg, ctx->d_sincos, d_cnl, r, k, nrays, seed, d_rays, st_col, st_val, row_nnz,
-                         ctx->d_flags, s));
+                         ctx->d_flags, s, ctx->d_flags + 4));
       int32_t flags = 0;
       RCU(cudaMemcpyAsync(&flags, ctx->d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
       RCU(cudaStreamSynchronize(s));
@@ -544,6 +544,7 @@ raptr_status run_build(raptr_ctx* ctx, const int32_t* d_cnl, int64_t n_list, int
   if (!out.rp) return fail(RAPTR_ERR_INVALID, "row pointer buffer is null");
   RCU(cudaMemsetAsync(ctx->d_i64, 0, sizeof(int64_t), s));
   RCU(cudaMemsetAsync(out.rp, 0, sizeof(int64_t), s));
+  RCU(cudaMemsetAsync(ctx->d_flags + 4, 0, 4 * sizeof(int32_t), s));  // rows left to the table, by reason
   out.n_list = n_list;
   Builder b{ctx, d_cnl, n_list, nrays, seed, d_rays, (flags & RAPTR_SM_KEEP_ZEROS) != 0, s, out};
   if (n_list > 0) {
@@ -555,6 +556,13 @@ raptr_status run_build(raptr_ctx* ctx, const int32_t* d_cnl, int64_t n_list, int
   }
   RCU(cudaStreamSynchronize(s));
   *nnz_out = b.total;
+  if (trace_on()) {
+    int32_t why[4] = {0, 0, 0, 0};
+    RCU(cudaMemcpy(why, ctx->d_flags + 4, sizeof(why), cudaMemcpyDeviceToHost));
+    trace("build: %lld rows, rows built with the hash table: %d without a slab axis, %d with windows over the "
+          "slot limit, %d with a ray outside its windows, %d with a slot outside the grid",
+          (long long)n_list, why[0], why[1], why[2], why[3]);
+  }
   if (b.total > out.cap && !out.grow) {
     return fail(RAPTR_ERR_CAPACITY, "matrix has " + std::to_string(b.total) + " entries, buffer holds " +
                                         std::to_string(out.cap));
@@ -1429,16 +1437,18 @@ raptr_status batch_args(raptr_ctx* ctx, int64_t m, int64_t n, int32_t K, int32_t
                         const int32_t* d_col, const void* d_val, const float* d_rscale, const int64_t* d_col_ptr,
                         const int32_t* d_row_idx, const void* d_tval, const int32_t* d_row_rank, const float* d_y,
                         const float* d_s, float* d_x, BatchArgs* a) {
-  if (!ctx || m < 0 || n <= 0 || K <= 0 || K > 4096 || (value_type != 0 && value_type != 1) || !d_row_ptr ||
-      !d_col_ptr || !d_y || !d_s || !d_x || (m > 0 && (!d_val || !d_tval)) || (value_type == 1 && m > 0 && !d_rscale))
+  if (!ctx || m < 0 || n <= 0 || K <= 0 || K > 4096 || value_type < 0 || value_type > 2 || !d_row_ptr ||
+      !d_col_ptr || !d_y || !d_s || !d_x || (m > 0 && (!d_val || !d_tval)) || (value_type >= 1 && m > 0 && !d_rscale))
     return fail(RAPTR_ERR_INVALID, "bad argument");
-  // the passes gather four frames at a time (16-byte loads of the images)
-  if ((reinterpret_cast<uintptr_t>(d_x) & 15u) != 0)
-    return fail(RAPTR_ERR_INVALID, "the images must be 16-byte aligned");
+  // the passes gather four frames at a time (16-byte loads of the images
+  // and measurements)
+  if ((reinterpret_cast<uintptr_t>(d_x) & 15u) != 0 || (reinterpret_cast<uintptr_t>(d_y) & 15u) != 0)
+    return fail(RAPTR_ERR_INVALID, "the images and measurements must be 16-byte aligned");
   a->m = m;
   a->n = n;
   a->K = K;
-  a->half = value_type == 1;
+  a->half = value_type >= 1;
+  a->lowp = value_type == 2;
   a->rp = d_row_ptr;
   a->col = d_col;
   a->val = d_val;
@@ -1478,17 +1488,23 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
   RCHECK(ctx->ensure_scratch(Carve::need({size_t(std::max<int64_t>(m, 1)) * n_frames * sizeof(float),
                                           size_t(n) * n_frames * sizeof(float), size_t(n_frames) * sizeof(double),
                                           size_t(n_frames) * sizeof(unsigned long long) * kBatchRowBlocks,
-                                          size_t(n) * std::min(kt, int(n_frames)) * sizeof(float)})));
+                                          size_t(n) * std::min(kt, int(n_frames)) * sizeof(float),
+                                          size_t(n) * n_frames * sizeof(uint16_t)})));
   Carve cv(ctx->d_scratch);
   // the tube order of the back pass applies when the columns are the
   // context's voxels
   if (n == int64_t(ctx->dg.n[0]) * ctx->dg.n[1] * ctx->dg.n[2]) RCU(ctx->col_order(&a.col_order));
-  a.E = cv.take<float>(size_t(std::max<int64_t>(m, 1)) * n_frames);
+  if (a.lowp) {
+    a.Eh = cv.take<uint16_t>(size_t(std::max<int64_t>(m, 1)) * n_frames);
+    a.Xh = cv.take<uint16_t>(size_t(n) * n_frames);
+  } else {
+    a.E = cv.take<float>(size_t(std::max<int64_t>(m, 1)) * n_frames);
+  }
   a.XX = cv.take<float>(size_t(n) * n_frames);
   double* acc = cv.take<double>(size_t(n_frames));
   unsigned long long* next = cv.take<unsigned long long>(size_t(n_frames) * kBatchRowBlocks);
   // the back pass in row-block groups when one tile's ratios exceed L2
-  if (m > 0 && double(m) * std::min(kt, int(n_frames)) * sizeof(float) > kBatchBlockingBytes) {
+  if (m > 0 && double(m) * std::min(kt, int(n_frames)) * (a.lowp ? 2.0 : 4.0) > kBatchBlockingBytes) {
     RCU(ctx->block_seg(d_col_ptr, d_row_idx, m, n, s, &a.seg));
     a.seg_blocks = kBatchRowBlocks;
     a.P = cv.take<float>(size_t(n) * std::min(kt, int(n_frames)));
@@ -1499,6 +1515,8 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
     for (auto& ev : evs) RCU(cudaEventCreate(&ev));
   }
   auto enqueue = [&](cudaStream_t q) -> cudaError_t {
+    cudaError_t perr = launch_batch_prepare(a, q);
+    if (perr != cudaSuccess) return perr;
     for (int32_t it = 0; it < n_iter; it++) {
       cudaError_t err = cudaSuccess;
       if (want_times) err = cudaEventRecord(evs[size_t(3 * it)], q);

@@ -589,7 +589,7 @@ __global__ void __launch_bounds__(T) sm_dense_kernel(DGeom g, const float2* __re
                                                      const int32_t* __restrict__ cnl_ids, int64_t row0, int nrays,
                                                      uint32_t seed, int32_t* __restrict__ st_col,
                                                      float* __restrict__ st_val, int32_t* __restrict__ row_nnz,
-                                                     int32_t* __restrict__ flags) {
+                                                     int32_t* __restrict__ flags, int32_t* __restrict__ reasons) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* acc = reinterpret_cast<float*>(smem);  // dense_slots(H) slots + the spare one
   int* keys = reinterpret_cast<int*>(smem);     // z slabs: the row's entries for the sort
@@ -639,7 +639,10 @@ __global__ void __launch_bounds__(T) sm_dense_kernel(DGeom g, const float2* __re
   __syncthreads();
   const int A = sax;
   if (A < 0) {
-    if (tid == 0) row_nnz[blockIdx.x] = kRowToTable;
+    if (tid == 0) {
+      row_nnz[blockIdx.x] = kRowToTable;
+      if (reasons) atomicAdd(reasons + 0, 1);
+    }
     return;
   }
   const int iu_ax = A == 0 ? 1 : 0, iv_ax = A == 0 ? 2 : 1;
@@ -661,7 +664,10 @@ __global__ void __launch_bounds__(T) sm_dense_kernel(DGeom g, const float2* __re
   const int wu = win_u, wv = win_v;
   const int wuv = wu * wv;
   if (!((long long)na * wuv < (long long)dense_slots(H))) {  // + the spare slot
-    if (tid == 0) row_nnz[blockIdx.x] = kRowToTable;
+    if (tid == 0) {
+      row_nnz[blockIdx.x] = kRowToTable;
+      if (reasons) atomicAdd(reasons + 1, 1);
+    }
     return;
   }
   const int nslots = na * wuv;
@@ -716,7 +722,10 @@ __global__ void __launch_bounds__(T) sm_dense_kernel(DGeom g, const float2* __re
   // a slot outside the windows was added to the spare slot: every thread
   // reads the same value and takes the same branch
   if (dense_fail || acc[nslots] != 0.f) {
-    if (tid == 0) row_nnz[blockIdx.x] = kRowToTable;
+    if (tid == 0) {
+      row_nnz[blockIdx.x] = kRowToTable;
+      if (reasons) atomicAdd(reasons + 2, 1);
+    }
     return;
   }
 
@@ -763,7 +772,10 @@ __global__ void __launch_bounds__(T) sm_dense_kernel(DGeom g, const float2* __re
   }
   __syncthreads();
   if (dense_fail) {
-    if (tid == 0) row_nnz[blockIdx.x] = kRowToTable;
+    if (tid == 0) {
+      row_nnz[blockIdx.x] = kRowToTable;
+      if (reasons) atomicAdd(reasons + 3, 1);
+    }
     return;
   }
   // Second pass: after a scan of the warp counts, each warp writes its
@@ -926,7 +938,7 @@ constexpr int kNumLevels = 4;
 template <int H, int T>
 cudaError_t launch_level(const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0, int64_t nrows,
                          int nrays, uint32_t seed, const float* d_rays, int32_t* st_col, float* st_val,
-                         int32_t* row_nnz, int32_t* d_flags, cudaStream_t s) {
+                         int32_t* row_nnz, int32_t* d_flags, int32_t* d_reasons, cudaStream_t s) {
   // A grid with the same origin on every axis (the usual centred cube) lets
   // the walk's step skip selecting the origin.
   const bool oiso = g.o[0] == g.o[1] && g.o[1] == g.o[2];
@@ -946,7 +958,7 @@ cudaError_t launch_level(const DGeom& g, const float2* d_sincos, const int32_t* 
   e = cudaFuncSetAttribute(dense, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dense_smem));
   if (e != cudaSuccess) return e;
   dense<<<unsigned(nrows), T, dense_smem, s>>>(g, d_sincos, d_cnl, row0, nrays, seed, st_col, st_val, row_nnz,
-                                               d_flags);
+                                               d_flags, d_reasons);
   // the rows the dense kernel left to the table (none on most workloads),
   // four blocks per SM looking through the row states
   const int64_t tb = std::min<int64_t>(nrows, 148 * 4);
@@ -1197,13 +1209,14 @@ int sm_pick_level(const DGeom& g, int nrays) {
 
 cudaError_t launch_sm_rows(int level, const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0,
                            int64_t nrows, int nrays, uint32_t seed, const float* d_rays, int32_t* st_col,
-                           float* st_val, int32_t* row_nnz, int32_t* d_flags, cudaStream_t s) {
+                           float* st_val, int32_t* row_nnz, int32_t* d_flags, cudaStream_t s,
+                           int32_t* d_table_reasons) {
   if (nrows <= 0) return cudaSuccess;
   switch (level) {
-    case 0: return launch_level<2048, 128>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, s);
-    case 1: return launch_level<4096, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, s);
-    case 2: return launch_level<8192, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, s);
-    case 3: return launch_level<16384, 512>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, s);
+    case 0: return launch_level<2048, 128>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, s);
+    case 1: return launch_level<4096, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, s);
+    case 2: return launch_level<8192, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, s);
+    case 3: return launch_level<16384, 512>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, s);
     default: return cudaErrorInvalidValue;
   }
 }
