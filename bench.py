@@ -419,36 +419,20 @@ def batch_report(R, torch, ctx, w, lst, plain_iters_per_s, peak, n_frames=64, ni
         lam = R.spmv(R.OP_N, A.m, A.n, A.row_ptr, A.col, A.val, (xt * torch.exp(-rates * f)).contiguous())
         Y[:, f] = torch.poisson(lam * (counts[f] / float(lam.double().sum())), generator=gen)
     h64, s16 = R.sensitivity_half(A)
+    X = torch.full((n, n_frames), np.float32(1.0 / n), device="cuda")
+    best, tile_ms = ctx.batch_autotune(A, Y, s16, X)
+    kt = ctx.mlem_batch(A, Y, s16, X.clone(), 3, frame_tile=best, use_graph=False, kernel_times=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    ctx.mlem_batch(A, Y, s16, X, niter, frame_tile=best, use_graph=True)
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1])
+    rate = n_frames * niter / (ms / 1e3)
     # frame 0 against the FP64 iteration on its own
     s64, _ = R.sensitivity(A)
     x64 = torch.full((n,), 1.0 / n, dtype=torch.float64, device="cuda")
     ctx.mlem_f64(A, Y[:, 0].contiguous(), s64 / s64.sum(), x64, niter)
-
-    def run(half):
-        X = torch.full((n, n_frames), np.float32(1.0 / n), device="cuda")
-        best, tile_ms = ctx.batch_autotune(A, Y, s16, X, half=half)
-        kt = ctx.mlem_batch(A, Y, s16, X.clone(), 3, frame_tile=best, half=half, use_graph=False, kernel_times=True)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        ev[0].record()
-        ctx.mlem_batch(A, Y, s16, X, niter, frame_tile=best, half=half, use_graph=True)
-        ev[1].record()
-        torch.cuda.synchronize()
-        return X, best, tile_ms, kt, ev[0].elapsed_time(ev[1])
-
-    # the bfloat16-gather form first (its result is reported beside the other)
-    Xb, best_b, tile_b, kt_b, ms_b = run("bf16")
-    d_b = Xb[:, 0].double() - x64
-    rate_b = n_frames * niter / (ms_b / 1e3)
-    bf16 = {"frame_tile": best_b, "autotune_ms_per_iteration": {str(k): round(v, 3) for k, v in tile_b.items()},
-            "frame_iterations_per_s": rate_b, "ms_per_iteration_all_frames": ms_b / niter,
-            "speedup_vs_plain_fp32_single_frame": rate_b / plain_iters_per_s,
-            "passes_ms": {"forward": round(float(kt_b[:, 0].mean()), 3), "back": round(float(kt_b[:, 1].mean()), 3)},
-            "frame0_vs_fp64": {"rel_l2": float(d_b.norm() / x64.norm()),
-                               "max_rel": float(d_b.abs().max() / x64.abs().max())},
-            "gathers": "images and ratios as bfloat16 (raptr_mlem_batch value_type 2)"}
-    del Xb
-    X, best, tile_ms, kt, ms = run(True)
-    rate = n_frames * niter / (ms / 1e3)
     d = X[:, 0].double() - x64
     fwd_ms, back_ms = float(kt[:, 0].mean()), float(kt[:, 1].mean())
     nnz, m = A.nnz, A.m
@@ -463,7 +447,6 @@ def batch_report(R, torch, ctx, w, lst, plain_iters_per_s, peak, n_frames=64, ni
         "gathered_gb_per_s": {"forward": round(nnz * n_frames * 4 / fwd_ms / 1e6, 1),
                               "back": round(nnz * n_frames * 4 / back_ms / 1e6, 1)},
         "frame0_vs_fp64": {"rel_l2": float(d.norm() / x64.norm()), "max_rel": float(d.abs().max() / x64.abs().max())},
-        "bf16_gathers": bf16,
         "data": "seeded per-voxel washout rates and log-uniform counts; Poisson via a seeded CUDA generator",
     }
     del A, Y, X
@@ -497,7 +480,7 @@ def streamed_report(R, torch, ctx, w, lst, y_dev, fraction=0.25, niter=3):
                     "staging in every iteration; the first iteration builds every row and the sensitivity"}
 
 
-def serving_report(R, torch, rate_hz=20.0, window_s=8.0, budget_gb=120, seed=SEED + 500, gathers="fp32"):
+def serving_report(R, torch, rate_hz=20.0, window_s=8.0, budget_gb=120, seed=SEED + 500):
     """The serving form: Poisson arrivals at rate_hz for window_s seconds of
     reconstructions drawn from three geometries (40^3 x 2 mm / 5 angles,
     70^3 x 2 mm / 180 angles, 100^3 x 1.5 mm / 60 angles), counts
@@ -528,7 +511,7 @@ def serving_report(R, torch, rate_hz=20.0, window_s=8.0, budget_gb=120, seed=SEE
         del lam
         torch.cuda.empty_cache()
     t_syn = time.perf_counter() - t_syn
-    srv = R.Server(0, hbm_budget_bytes=int(budget_gb) << 30, gathers=gathers)
+    srv = R.Server(0, hbm_budget_bytes=int(budget_gb) << 30)
     warm = {}
     for name, w in sorted(kinds, key=lambda kv: -kv[1]["geom"].n_channels):
         g = w["geom"]
@@ -577,7 +560,7 @@ def serving_report(R, torch, rate_hz=20.0, window_s=8.0, budget_gb=120, seed=SEE
         "by_geometry": by, "warm_first_request_ms": warm,
         "server": {k: stats[k] for k in ("builds", "evictions", "batch_steps", "iterations")},
         "largest_batch": int(max(st["frames_max"] for _, _, st in results)),
-        "hbm_budget_gb": budget_gb, "synthesis_s": t_syn, "gathers": gathers,
+        "hbm_budget_gb": budget_gb, "synthesis_s": t_syn,
         "accuracy": "batched FP16 iteration; equal alone and in the mix and within 1e-3 of FP64 (tests/test_gpu_server.py)",
     }
 
@@ -754,9 +737,8 @@ def main():
         del lst, y_dev
         gc.collect()
         torch.cuda.empty_cache()
-        out["forms"]["serving"] = {
-            "offered_20_per_s": serving_report(R, torch, rate_hz=20.0, window_s=30.0, gathers="bf16"),
-            "offered_12_per_s": serving_report(R, torch, rate_hz=12.0, window_s=20.0, gathers="bf16")}
+        out["forms"]["serving"] = {"offered_20_per_s": serving_report(R, torch, rate_hz=20.0, window_s=30.0),
+                                   "offered_8_per_s": serving_report(R, torch, rate_hz=8.0, window_s=20.0)}
     if rank == 0 and world == 1:
         out["cpu_baseline"] = {k: v for k, v in cpu_job_rate(w, args.cpu_sample_s, os.cpu_count() or 1).items()
                                if k != "matrix_build_s"}

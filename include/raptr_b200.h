@@ -329,11 +329,8 @@ raptr_status raptr_mlem_f64(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t*
  * d_s is the one normalised sensitivity; each frame's image is normalised
  * to sum 1 after every iteration.  The matrix is FP32 (value_type 0: d_val /
  * d_tval float) or the FP16 form (value_type 1: d_val = hval, d_tval =
- * htval, d_rscale the row scales); value_type 2 is the FP16 form with the
- * images and ratios gathered as bfloat16 (half the gathered bytes; each
- * frame's image stays within 1e-3 of the FP64 iteration, and depends on no
- * other frame).  The transpose is required and d_row_rank follows it
- * (raptr_matrix_row_order, may be null for the natural order).  When one
+ * htval, d_rscale the row scales).  The transpose is required and d_row_rank
+ * follows it (raptr_matrix_row_order, may be null for the natural order).  When one
  * frame tile's ratios exceed ~96 MB, the back pass runs over groups of row
  * blocks of the transpose so that the ratios it gathers stay in L2.
  * n_frames must be a multiple of 4.  Each pass handles up to frame_tile
@@ -428,9 +425,6 @@ typedef struct raptr_server_opts {
                                a build's transient memory (~24 bytes/entry)   */
   int32_t max_frames;       /* requests per geometry batch, 1..64              */
   int32_t keep_fp32;        /* keep the FP32 values of cached matrices         */
-  int32_t gathers;          /* 0: batches gather FP32 images and ratios
-                               (raptr_mlem_batch value_type 1); 1: bfloat16
-                               (value_type 2, half the gathered bytes)        */
 } raptr_server_opts;
 typedef struct raptr_request_stats {
   double queue_ms;   /* submit -> admitted                                    */

@@ -59,8 +59,7 @@ class raptr_mlem_opts(C.Structure):
 
 
 class raptr_server_opts(C.Structure):
-    _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_frames", C.c_int32), ("keep_fp32", C.c_int32),
-                ("gathers", C.c_int32)]
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_frames", C.c_int32), ("keep_fp32", C.c_int32)]
 
 
 class raptr_request_stats(C.Structure):
@@ -467,18 +466,16 @@ class Context:
             out.append(np.array(kt[:2 * niter], np.float64).reshape(niter, 2))
         return None if not out else (out[0] if len(out) == 1 else tuple(out))
 
-    def _batch_arrays(self, A: Matrix, half):
-        """half: False (FP32 matrix), True (FP16 matrix) or "bf16" (FP16
-        matrix, images and ratios gathered as bfloat16)."""
+    def _batch_arrays(self, A: Matrix, half: bool):
         if not A.has_transpose:
             A.transpose()
         if half:
             if A.hval is None:
                 A.to_half()
-            return (2 if half == "bf16" else 1), _ptr(A.hval), _ptr(A.rscale), _ptr(A.htval)
+            return 1, _ptr(A.hval), _ptr(A.rscale), _ptr(A.htval)
         return 0, _ptr(A.val), None, _ptr(A.tval)
 
-    def mlem_batch(self, A: Matrix, Y, s, X, niter: int, frame_tile: int = 0, half=True,
+    def mlem_batch(self, A: Matrix, Y, s, X, niter: int, frame_tile: int = 0, half: bool = True,
                    use_graph: bool = True, kernel_times: bool = False, stream=None):
         """MLEM for K frames together: Y (m, K) and X (n, K) float32,
         row-major (frame-minor); s the one normalised sensitivity.  Returns
@@ -494,7 +491,7 @@ class Context:
                                       _ptr(X), niter, frame_tile, C.byref(opts), _stream(stream)))
         return np.array(kt[:2 * niter], np.float64).reshape(niter, 2) if kernel_times else None
 
-    def batch_autotune(self, A: Matrix, Y, s, X, half=True, stream=None):
+    def batch_autotune(self, A: Matrix, Y, s, X, half: bool = True, stream=None):
         """(best frame tile, {tile: ms per iteration}) for these frames."""
         K = int(X.shape[1])
         vt, val, rsc, tval = self._batch_arrays(A, half)
@@ -524,11 +521,8 @@ class Server:
     matrices cached in HBM."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 100 << 30, max_frames: int = 64,
-                 keep_fp32: bool = False, gathers: str = "fp32"):
-        """gathers: "fp32" or "bf16" (the batches gather images and ratios as
-        bfloat16: raptr_mlem_batch value_type 2)."""
-        o = raptr_server_opts(int(hbm_budget_bytes), int(max_frames), 1 if keep_fp32 else 0,
-                              1 if gathers == "bf16" else 0)
+                 keep_fp32: bool = False):
+        o = raptr_server_opts(int(hbm_budget_bytes), int(max_frames), 1 if keep_fp32 else 0)
         h = VP()
         _check(lib().raptr_server_create(device, C.byref(o), C.byref(h)))
         self._h = h

@@ -348,7 +348,8 @@ struct Builder {
     int64_t per = std::max<int64_t>(1, int64_t(kStagingBudget / (size_t(H) * 8)));
     per = std::min<int64_t>(per, 65536);
     if (!ctx->h_pin) RCU(cudaMallocHost(&ctx->h_pin, 16 * sizeof(int64_t)));
-    volatile int32_t* h_flags = reinterpret_cast<volatile int32_t*>(ctx->h_pin);  // 2 words
+    // words 0-1: the dense kernel's flags, 2-3: the table kernel's (per buffer)
+    volatile int32_t* h_flags = reinterpret_cast<volatile int32_t*>(ctx->h_pin);
     volatile int64_t* h_total = ctx->h_pin + 2;
     cudaStream_t P = nullptr;
     cudaEvent_t ev_k[2] = {nullptr, nullptr}, ev_g[2] = {nullptr, nullptr}, ev_j = nullptr;
@@ -401,7 +402,7 @@ struct Builder {
         if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_flags + b, 0, sizeof(int32_t), s);
         if (e == cudaSuccess)
           e = launch_sm_rows(level, ctx->dg, ctx->d_sincos, d_cnl, r, k, nrays, seed, d_rays, st_col[b], st_val[b],
-                             row_nnz[b], ctx->d_flags + b, s, ctx->d_flags + 4);
+                             row_nnz[b], ctx->d_flags + b, s, ctx->d_flags + 4, d_rays ? kRowsAll : kRowsDense);
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(const_cast<int32_t*>(h_flags) + b, ctx->d_flags + b, sizeof(int32_t),
                               cudaMemcpyDeviceToHost, s);
@@ -439,6 +440,37 @@ struct Builder {
           break;
         }
         e = cudaStreamWaitEvent(P, ev_k[b], 0);
+        if (!d_rays) {
+          // The rows the dense kernel left to the hash table, on the
+          // placement stream: a row or two per chunk, which would otherwise
+          // hold up the next chunk's dense rows on the caller's stream.
+          if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_flags + 2 + b, 0, sizeof(int32_t), P);
+          if (e == cudaSuccess)
+            e = launch_sm_rows(level, ctx->dg, ctx->d_sincos, d_cnl, r, k, nrays, seed, nullptr, st_col[b],
+                               st_val[b], row_nnz[b], ctx->d_flags + 2 + b, P, nullptr, kRowsTable);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(const_cast<int32_t*>(h_flags) + 2 + b, ctx->d_flags + 2 + b, sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, P);
+          if (e == cudaSuccess) e = cudaStreamSynchronize(P);
+          if (e != cudaSuccess) {
+            drain();
+            return cuda_fail(e, "system-matrix rows (table)");
+          }
+          const int32_t tflags = h_flags[2 + b];
+          if (tflags & 6) {
+            RCU(drain());
+            if (tflags & 4) return fail(RAPTR_ERR_INVALID, "a channel id is outside [0, number of channels)");
+            return fail(RAPTR_ERR_OVERFLOW, "ray walk did not terminate (internal error)");
+          }
+          if (tflags & 1) {
+            RCU(drain());
+            if (level + 1 >= sm_num_levels())
+              return fail(RAPTR_ERR_OVERFLOW, "a row has more distinct voxels than the largest per-row table holds");
+            RCHECK(rows(level + 1, r, k));
+            next_r0 = r + k;
+            break;
+          }
+        }
         if (e == cudaSuccess) e = launch_rows_scan(row_nnz[b], k, out.rp + r, ctx->d_i64, P);
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(const_cast<int64_t*>(h_total), ctx->d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, P);
@@ -1437,8 +1469,8 @@ raptr_status batch_args(raptr_ctx* ctx, int64_t m, int64_t n, int32_t K, int32_t
                         const int32_t* d_col, const void* d_val, const float* d_rscale, const int64_t* d_col_ptr,
                         const int32_t* d_row_idx, const void* d_tval, const int32_t* d_row_rank, const float* d_y,
                         const float* d_s, float* d_x, BatchArgs* a) {
-  if (!ctx || m < 0 || n <= 0 || K <= 0 || K > 4096 || value_type < 0 || value_type > 2 || !d_row_ptr ||
-      !d_col_ptr || !d_y || !d_s || !d_x || (m > 0 && (!d_val || !d_tval)) || (value_type >= 1 && m > 0 && !d_rscale))
+  if (!ctx || m < 0 || n <= 0 || K <= 0 || K > 4096 || (value_type != 0 && value_type != 1) || !d_row_ptr ||
+      !d_col_ptr || !d_y || !d_s || !d_x || (m > 0 && (!d_val || !d_tval)) || (value_type == 1 && m > 0 && !d_rscale))
     return fail(RAPTR_ERR_INVALID, "bad argument");
   // the passes gather four frames at a time (16-byte loads of the images
   // and measurements)
@@ -1447,8 +1479,7 @@ raptr_status batch_args(raptr_ctx* ctx, int64_t m, int64_t n, int32_t K, int32_t
   a->m = m;
   a->n = n;
   a->K = K;
-  a->half = value_type >= 1;
-  a->lowp = value_type == 2;
+  a->half = value_type == 1;
   a->rp = d_row_ptr;
   a->col = d_col;
   a->val = d_val;
@@ -1488,23 +1519,17 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
   RCHECK(ctx->ensure_scratch(Carve::need({size_t(std::max<int64_t>(m, 1)) * n_frames * sizeof(float),
                                           size_t(n) * n_frames * sizeof(float), size_t(n_frames) * sizeof(double),
                                           size_t(n_frames) * sizeof(unsigned long long) * kBatchRowBlocks,
-                                          size_t(n) * std::min(kt, int(n_frames)) * sizeof(float),
-                                          size_t(n) * n_frames * sizeof(uint16_t)})));
+                                          size_t(n) * std::min(kt, int(n_frames)) * sizeof(float)})));
   Carve cv(ctx->d_scratch);
   // the tube order of the back pass applies when the columns are the
   // context's voxels
   if (n == int64_t(ctx->dg.n[0]) * ctx->dg.n[1] * ctx->dg.n[2]) RCU(ctx->col_order(&a.col_order));
-  if (a.lowp) {
-    a.Eh = cv.take<uint16_t>(size_t(std::max<int64_t>(m, 1)) * n_frames);
-    a.Xh = cv.take<uint16_t>(size_t(n) * n_frames);
-  } else {
-    a.E = cv.take<float>(size_t(std::max<int64_t>(m, 1)) * n_frames);
-  }
+  a.E = cv.take<float>(size_t(std::max<int64_t>(m, 1)) * n_frames);
   a.XX = cv.take<float>(size_t(n) * n_frames);
   double* acc = cv.take<double>(size_t(n_frames));
   unsigned long long* next = cv.take<unsigned long long>(size_t(n_frames) * kBatchRowBlocks);
   // the back pass in row-block groups when one tile's ratios exceed L2
-  if (m > 0 && double(m) * std::min(kt, int(n_frames)) * (a.lowp ? 2.0 : 4.0) > kBatchBlockingBytes) {
+  if (m > 0 && double(m) * std::min(kt, int(n_frames)) * sizeof(float) > kBatchBlockingBytes) {
     RCU(ctx->block_seg(d_col_ptr, d_row_idx, m, n, s, &a.seg));
     a.seg_blocks = kBatchRowBlocks;
     a.P = cv.take<float>(size_t(n) * std::min(kt, int(n_frames)));
@@ -1515,8 +1540,6 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
     for (auto& ev : evs) RCU(cudaEventCreate(&ev));
   }
   auto enqueue = [&](cudaStream_t q) -> cudaError_t {
-    cudaError_t perr = launch_batch_prepare(a, q);
-    if (perr != cudaSuccess) return perr;
     for (int32_t it = 0; it < n_iter; it++) {
       cudaError_t err = cudaSuccess;
       if (want_times) err = cudaEventRecord(evs[size_t(3 * it)], q);

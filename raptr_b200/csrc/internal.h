@@ -53,11 +53,15 @@ int sm_pick_level(const DGeom& g, int nrays);
 // overflowed.  *d_flags |= 1 on overflow, |= 4 for a channel id out of range.
 // With d_table_reasons (4 ints) the rows the dense kernel leaves to the hash
 // table are counted by reason: no slab axis, windows over the slot limit,
-// a ray outside the windows, a slot decoding outside the grid.
+// a ray outside the windows, a slot decoding outside the grid.  parts: 1 =
+// the dense kernel only (rows it cannot take keep row_nnz = -2), 2 = the
+// table kernel for those rows only, 3 = both; with d_rays every row takes
+// the table kernel whatever parts says.
+constexpr int kRowsDense = 1, kRowsTable = 2, kRowsAll = 3;
 cudaError_t launch_sm_rows(int level, const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0,
                            int64_t nrows, int nrays, uint32_t seed, const float* d_rays, int32_t* st_col,
                            float* st_val, int32_t* row_nnz, int32_t* d_flags, cudaStream_t s,
-                           int32_t* d_table_reasons = nullptr);
+                           int32_t* d_table_reasons = nullptr, int parts = kRowsAll);
 
 // Exclusive scan of row_nnz[0..n) into row_ptr[0..n] (int64) starting at
 // *d_base; *d_base is advanced by the sum.  One block.
@@ -192,15 +196,7 @@ struct BatchArgs {
   const int32_t* seg = nullptr;
   int seg_blocks = 0;
   float* P = nullptr;
-  // Reduced-precision gathers: the forward pass gathers the bfloat16 copy
-  // Xh (n x K) of the images and stores the ratios as bfloat16 Eh (m x K),
-  // which the back pass gathers; X, XX and the sums stay FP32.
-  bool lowp = false;
-  uint16_t* Xh = nullptr;
-  uint16_t* Eh = nullptr;
 };
-// Before the first iteration of a call: the bfloat16 copy of the images.
-cudaError_t launch_batch_prepare(const BatchArgs& a, cudaStream_t s);
 // The row-block offsets of every column of a transpose (see BatchArgs.seg):
 // seg[j*(B+1) + b] = offset in column j of its first entry with row >= b*m/B.
 cudaError_t launch_block_seg(int64_t n, int64_t m, int B, const int64_t* cp, const int32_t* trow, int32_t* seg,

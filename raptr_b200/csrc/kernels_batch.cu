@@ -18,7 +18,6 @@
 #include <cstdint>
 #include <vector>
 
-#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "internal.h"
@@ -55,27 +54,6 @@ struct Split {
 
 __device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
-// Four bfloat16 values (one 8-byte load) as floats: a bfloat16 is the high
-// half of a float's bits.
-__device__ __forceinline__ float4 ld4(const uint16_t* p) {
-  const uint2 w = __ldg(reinterpret_cast<const uint2*>(p));
-  return make_float4(__uint_as_float(w.x << 16), __uint_as_float(w.x & 0xffff0000u), __uint_as_float(w.y << 16),
-                     __uint_as_float(w.y & 0xffff0000u));
-}
-
-// Round to nearest even bfloat16 (bits).
-__device__ __forceinline__ uint32_t bf16_bits(float v) {
-  return uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(v)));
-}
-
-__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
-  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-}
-__device__ __forceinline__ void st4(uint16_t* p, const float (&v)[4]) {
-  *reinterpret_cast<uint2*>(p) = make_uint2(bf16_bits(v[0]) | (bf16_bits(v[1]) << 16),
-                                            bf16_bits(v[2]) | (bf16_bits(v[3]) << 16));
-}
-
 __device__ __forceinline__ void fma4(float (&a)[4], float w, float4 x) {
   a[0] += w * x.x;
   a[1] += w * x.y;
@@ -85,18 +63,16 @@ __device__ __forceinline__ void fma4(float (&a)[4], float w, float4 x) {
 
 // Forward: E[rank_i*K + f] = sc_i * Y[i*K + f] / (sc_i * sum_j v_ij X[j*K + f])
 // for the frames f of the tile (0 where Y == 0); sc = rscale (FP16) or 1.
-// GT is the type the images are gathered in and the ratios stored in:
-// float, or bfloat16 (uint16_t bits) in the reduced-precision form.
-template <int KT, typename VT, typename GT>
+template <int KT, typename VT>
 __global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int K, int f0,
                                                                  const int64_t* __restrict__ rp,
                                                                  const int32_t* __restrict__ col,
                                                                  const VT* __restrict__ val,
                                                                  const float* __restrict__ rscale,
                                                                  const float* __restrict__ Y,
-                                                                 const GT* __restrict__ X,
+                                                                 const float* __restrict__ X,
                                                                  const int32_t* __restrict__ rank,
-                                                                 GT* __restrict__ E) {
+                                                                 float* __restrict__ E) {
   using S = Split<KT>;
   const int lane = threadIdx.x & 31;
   const int es = lane / S::LPE, fg = lane % S::LPE;
@@ -125,12 +101,11 @@ __global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int 
     if (es == 0) {
       const float sc = rscale ? __ldg(rscale + r) : 1.f;
       const int64_t dst = rank ? int64_t(__ldg(rank + r)) : r;
-      const float4 y4 = ld4(Y + r * K + fbase);
-      const float yv[4] = {y4.x, y4.y, y4.z, y4.w};
-      float ev[4];
 #pragma unroll
-      for (int v = 0; v < S::VEC; v++) ev[v] = yv[v] == 0.f ? 0.f : sc * __fdiv_rn(yv[v], sc * acc[v]);
-      st4(E + dst * K + fbase, ev);
+      for (int v = 0; v < S::VEC; v++) {
+        const float yi = __ldg(Y + r * K + fbase + v);
+        E[dst * K + fbase + v] = yi == 0.f ? 0.f : sc * __fdiv_rn(yi, sc * acc[v]);
+      }
     }
   }
 }
@@ -147,12 +122,12 @@ __global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int 
 // sums of all but the last group go to P (n x KT, tile-local frames); the
 // last group adds them and finishes as above.  mode: 0 = the whole column
 // at once, 1 = first group, 2 = a middle group, 3 = the last group.
-template <int KT, typename VT, typename GT>
+template <int KT, typename VT>
 __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, int f0, unsigned long long* next,
                                                               const int64_t* __restrict__ cp,
                                                               const int32_t* __restrict__ trow,
                                                               const VT* __restrict__ tval,
-                                                              const GT* __restrict__ E,
+                                                              const float* __restrict__ E,
                                                               const float* __restrict__ X,
                                                               const float* __restrict__ sens,
                                                               const int32_t* __restrict__ col_order,
@@ -235,22 +210,14 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
     if (red[i] != 0.0) atomicAdd(acc + f0 + i, red[i]);
 }
 
-// X = XX * (1 / acc[f]) for all frames, and its bfloat16 copy Xh when
-// given (the images the reduced-precision forward pass gathers).
+// X = XX * (1 / acc[f]) for all frames; then acc = 0 for the next pass.
 __global__ void batch_normalise_kernel(int64_t n, int K, float* __restrict__ X, const float* __restrict__ XX,
-                                       const double* __restrict__ acc, uint16_t* __restrict__ Xh) {
+                                       const double* __restrict__ acc) {
   const int64_t total = n * K;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
     const int f = int(i % K);
-    const float x = XX[i] * float(1.0 / acc[f]);
-    X[i] = x;
-    if (Xh) Xh[i] = uint16_t(bf16_bits(x));
+    X[i] = XX[i] * float(1.0 / acc[f]);
   }
-}
-
-__global__ void to_bf16_kernel(int64_t total, const float* __restrict__ X, uint16_t* __restrict__ Xh) {
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x)
-    Xh[i] = uint16_t(bf16_bits(X[i]));
 }
 
 // A back pass over row blocks [b0, b1) of the transpose (mode as in
@@ -259,26 +226,19 @@ struct BackGroup {
   int b0 = 0, b1 = 0, mode = 0;
 };
 
-template <int KT, typename VT, typename GT>
-cudaError_t launch_tile_g(const BatchArgs& a, const GT* Xg, GT* E, bool forward, int f0, double* acc,
-                          unsigned long long* next, const BackGroup& grp, cudaStream_t s) {
-  if (forward)
-    batch_forward_kernel<KT, VT, GT><<<grid_warps(a.m), kThreads, 0, s>>>(
-        a.m, a.K, f0, a.rp, a.col, static_cast<const VT*>(a.val), a.half ? a.rscale : nullptr, a.Y, Xg, a.rank, E);
-  else
-    batch_back_kernel<KT, VT, GT>
-        <<<unsigned((a.n + kColsPerWarp * (kThreads / 32) - 1) / (kColsPerWarp * (kThreads / 32))), kThreads, 0, s>>>(
-            a.n, a.K, f0, next, a.cp, a.trow, static_cast<const VT*>(a.tval), E, a.X, a.S, a.col_order, a.XX, acc,
-            grp.mode ? a.seg : nullptr, a.seg_blocks + 1, grp.b0, grp.b1, grp.mode, a.P);
-  note_launches(1);
-  return cudaGetLastError();
-}
-
 template <int KT, typename VT>
 cudaError_t launch_tile(const BatchArgs& a, bool forward, int f0, double* acc, unsigned long long* next,
                         const BackGroup& grp, cudaStream_t s) {
-  if (a.lowp) return launch_tile_g<KT, VT, uint16_t>(a, a.Xh, a.Eh, forward, f0, acc, next, grp, s);
-  return launch_tile_g<KT, VT, float>(a, a.X, a.E, forward, f0, acc, next, grp, s);
+  if (forward)
+    batch_forward_kernel<KT, VT><<<grid_warps(a.m), kThreads, 0, s>>>(
+        a.m, a.K, f0, a.rp, a.col, static_cast<const VT*>(a.val), a.half ? a.rscale : nullptr, a.Y, a.X, a.rank, a.E);
+  else
+    batch_back_kernel<KT, VT><<<unsigned((a.n + kColsPerWarp * (kThreads / 32) - 1) / (kColsPerWarp * (kThreads / 32))),
+                                kThreads, 0, s>>>(a.n, a.K, f0, next, a.cp, a.trow, static_cast<const VT*>(a.tval), a.E,
+                                                  a.X, a.S, a.col_order, a.XX, acc, grp.mode ? a.seg : nullptr,
+                                                  a.seg_blocks + 1, grp.b0, grp.b1, grp.mode, a.P);
+  note_launches(1);
+  return cudaGetLastError();
 }
 
 template <typename VT>
@@ -318,16 +278,6 @@ __global__ void block_seg_kernel(int64_t n, int64_t m, int B, const int64_t* __r
 
 }  // namespace
 
-cudaError_t launch_batch_prepare(const BatchArgs& a, cudaStream_t s) {
-  if (!a.lowp) return cudaSuccess;
-  const int64_t total = a.n * a.K;
-  int64_t blocks = (total + kThreads - 1) / kThreads;
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  to_bf16_kernel<<<unsigned(std::max<int64_t>(blocks, 1)), kThreads, 0, s>>>(total, a.X, a.Xh);
-  note_launches(1);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_block_seg(int64_t n, int64_t m, int B, const int64_t* cp, const int32_t* trow, int32_t* seg,
                              cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
@@ -360,7 +310,7 @@ cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, unsi
       out.push_back(BackGroup{});
       return out;
     }
-    const double block_bytes = double(a.m) / a.seg_blocks * t * (a.lowp ? 2.0 : 4.0);
+    const double block_bytes = double(a.m) / a.seg_blocks * t * sizeof(float);
     const int g = std::max(1, int(kBackGroupBytes / std::max(block_bytes, 1.0)));
     if (g >= a.seg_blocks) {
       out.push_back(BackGroup{});
@@ -400,7 +350,7 @@ cudaError_t launch_batch_iteration(const BatchArgs& a, int kt, double* acc, unsi
     const int64_t total = a.n * a.K;
     int64_t blocks = (total + kThreads - 1) / kThreads;
     if (blocks > 148 * 8) blocks = 148 * 8;
-    batch_normalise_kernel<<<unsigned(blocks), kThreads, 0, s>>>(a.n, a.K, a.X, a.XX, acc, a.lowp ? a.Xh : nullptr);
+    batch_normalise_kernel<<<unsigned(blocks), kThreads, 0, s>>>(a.n, a.K, a.X, a.XX, acc);
     note_launches(1);
     e = cudaGetLastError();
   }

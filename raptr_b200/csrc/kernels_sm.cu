@@ -938,7 +938,7 @@ constexpr int kNumLevels = 4;
 template <int H, int T>
 cudaError_t launch_level(const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0, int64_t nrows,
                          int nrays, uint32_t seed, const float* d_rays, int32_t* st_col, float* st_val,
-                         int32_t* row_nnz, int32_t* d_flags, int32_t* d_reasons, cudaStream_t s) {
+                         int32_t* row_nnz, int32_t* d_flags, int32_t* d_reasons, int parts, cudaStream_t s) {
   // A grid with the same origin on every axis (the usual centred cube) lets
   // the walk's step skip selecting the origin.
   const bool oiso = g.o[0] == g.o[1] && g.o[1] == g.o[2];
@@ -953,18 +953,24 @@ cudaError_t launch_level(const DGeom& g, const float2* d_sincos, const int32_t* 
     note_launches(1);
     return cudaGetLastError();
   }
-  auto dense = oiso ? sm_dense_kernel<H, T, true> : sm_dense_kernel<H, T, false>;
-  const size_t dense_smem = row_smem_bytes(H);
-  e = cudaFuncSetAttribute(dense, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dense_smem));
-  if (e != cudaSuccess) return e;
-  dense<<<unsigned(nrows), T, dense_smem, s>>>(g, d_sincos, d_cnl, row0, nrays, seed, st_col, st_val, row_nnz,
-                                               d_flags, d_reasons);
-  // the rows the dense kernel left to the table (none on most workloads),
-  // four blocks per SM looking through the row states
-  const int64_t tb = std::min<int64_t>(nrows, 148 * 4);
-  table<<<unsigned(tb), T, table_smem, s>>>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, nullptr, st_col, st_val,
-                                            row_nnz, d_flags, 1);
-  note_launches(2);
+  if (parts & 1) {
+    auto dense = oiso ? sm_dense_kernel<H, T, true> : sm_dense_kernel<H, T, false>;
+    const size_t dense_smem = row_smem_bytes(H);
+    e = cudaFuncSetAttribute(dense, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dense_smem));
+    if (e != cudaSuccess) return e;
+    dense<<<unsigned(nrows), T, dense_smem, s>>>(g, d_sincos, d_cnl, row0, nrays, seed, st_col, st_val, row_nnz,
+                                                 d_flags, d_reasons);
+    note_launches(1);
+  }
+  if (parts & 2) {
+    // the rows the dense kernel left to the table (a few per million on
+    // the centred-cube workloads), four blocks per SM looking through the
+    // row states
+    const int64_t tb = std::min<int64_t>(nrows, 148 * 4);
+    table<<<unsigned(tb), T, table_smem, s>>>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, nullptr, st_col,
+                                              st_val, row_nnz, d_flags, 1);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
@@ -1210,13 +1216,13 @@ int sm_pick_level(const DGeom& g, int nrays) {
 cudaError_t launch_sm_rows(int level, const DGeom& g, const float2* d_sincos, const int32_t* d_cnl, int64_t row0,
                            int64_t nrows, int nrays, uint32_t seed, const float* d_rays, int32_t* st_col,
                            float* st_val, int32_t* row_nnz, int32_t* d_flags, cudaStream_t s,
-                           int32_t* d_table_reasons) {
+                           int32_t* d_table_reasons, int parts) {
   if (nrows <= 0) return cudaSuccess;
   switch (level) {
-    case 0: return launch_level<2048, 128>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, s);
-    case 1: return launch_level<4096, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, s);
-    case 2: return launch_level<8192, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, s);
-    case 3: return launch_level<16384, 512>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, s);
+    case 0: return launch_level<2048, 128>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, parts, s);
+    case 1: return launch_level<4096, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, parts, s);
+    case 2: return launch_level<8192, 256>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, parts, s);
+    case 3: return launch_level<16384, 512>(g, d_sincos, d_cnl, row0, nrows, nrays, seed, d_rays, st_col, st_val, row_nnz, d_flags, d_table_reasons, parts, s);
     default: return cudaErrorInvalidValue;
   }
 }

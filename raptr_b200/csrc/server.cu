@@ -496,11 +496,9 @@ void raptr_server::loop() {
         e->launch_status = RAPTR_ERR_NOMEM;
         e->launch_error = "batch relayout failed";
       } else {
-        // all frames (a multiple of 4) in as few sweeps of the matrix as the
-        // frame tiles allow
-        e->launch_status = raptr_mlem_batch(e->ctx, e->m, e->n, e->K, opts.gathers == 1 ? 2 : 1, e->rp, e->col,
-                                            e->hval, e->rscale, e->cp,
-                                            e->trow, e->htval, e->rank, e->Y, e->s, e->X(), 1, 64, nullptr,
+        // all frames in sweeps of at most 32 (a multiple of 4 frames)
+        e->launch_status = raptr_mlem_batch(e->ctx, e->m, e->n, e->K, 1, e->rp, e->col, e->hval, e->rscale, e->cp,
+                                            e->trow, e->htval, e->rank, e->Y, e->s, e->X(), 1, 32, nullptr,
                                             e->stream);
         if (e->launch_status != RAPTR_OK) e->launch_error = raptr_last_error();
       }
@@ -580,8 +578,7 @@ void raptr_server::loop() {
 extern "C" {
 
 raptr_status raptr_server_create(int32_t device, const raptr_server_opts* opts, raptr_server** out) {
-  if (!out || !opts || opts->hbm_budget_bytes <= 0 || opts->max_frames < 1 || opts->max_frames > 64 ||
-      opts->gathers < 0 || opts->gathers > 1)
+  if (!out || !opts || opts->hbm_budget_bytes <= 0 || opts->max_frames < 1 || opts->max_frames > 64)
     return set_error(RAPTR_ERR_INVALID, "bad server options");
   *out = nullptr;
   int ndev = 0;

@@ -167,24 +167,3 @@ def test_many_requests_join_and_leave(rlib, torch):
         frames.append(st["frames_max"])
     assert max(frames[:40]) > 32  # batches above 32 frames ran
     assert min(frames[40:]) > 1   # the late requests ran beside others
-
-
-def test_bfloat16_gathers_alone_mix_and_fp64(rlib, torch, jobs):
-    """Server with the batches' images and ratios gathered as bfloat16:
-    each result is the same alone and in a mix (1e-5) and within 1e-3 of
-    the FP64 iteration."""
-    srv = rlib.Server(0, hbm_budget_bytes=20 << 30, gathers="bf16")
-    alone = [srv.wait(srv.submit(g, y, it, NRAYS, SEED), g.n_voxels)[0] for g, it, y in jobs]
-    ids = [srv.submit(g, y, it, NRAYS, SEED) for g, it, y in jobs]
-    mixed = [srv.wait(rid, g.n_voxels)[0] for (g, it, y), rid in zip(jobs, ids)]
-    srv.close()
-    for xa, xm in zip(alone, mixed):
-        assert rel(xm, xa.astype(np.float64)) < MIX_RTOL
-    g, it, y = jobs[0]
-    ctx = rlib.Context(g, 0)
-    A = ctx.build(np.arange(g.n_channels, dtype=np.int32), NRAYS, SEED)
-    A.transpose()
-    s64, _ = rlib.sensitivity(A)
-    x64 = torch.full((A.n,), 1.0 / A.n, dtype=torch.float64, device="cuda")
-    ctx.mlem_f64(A, torch.from_numpy(y).cuda(), s64 / s64.sum(), x64, it)
-    assert rel(mixed[0], x64.cpu().numpy()) < F64_RTOL
