@@ -1218,28 +1218,34 @@ raptr_status mlem_impl(raptr_ctx* ctx, int64_t m, int64_t n, const MlemArrays& A
     for (auto& ev : evs) RCU(cudaEventCreate(&ev));
   }
   RCHECK(ctx->ensure_scratch(Carve::need({size_t(n) * sizeof(float), size_t(csc ? m : 1) * sizeof(float),
-                                          size_t(2 * n_iter + 2) * sizeof(double)})));
+                                          size_t(2 * n_iter + 4) * sizeof(double)})));
   Carve cv(ctx->d_scratch);
   float* c = cv.take<float>(size_t(n));  // correction (scatter path) or x before normalisation
   float* e = cv.take<float>(size_t(csc ? m : 1));
-  double* acc = cv.take<double>(size_t(2 * n_iter + 2));
-  double* ll = acc + 2;
+  double* acc = cv.take<double>(size_t(2 * n_iter + 4));
+  // acc[0]: the image sum; acc[1], acc[2]: the counters the forward and
+  // back passes draw rows and columns from (all three cleared in every
+  // iteration); from acc[4]: log-likelihood sums
+  auto* next_row = reinterpret_cast<unsigned long long*>(acc + 1);
+  auto* next_col = reinterpret_cast<unsigned long long*>(acc + 2);
+  double* ll = acc + 4;
   RCU(cudaMemsetAsync(c, 0, size_t(n) * sizeof(float), s));
-  RCU(cudaMemsetAsync(acc, 0, size_t(2 * n_iter + 2) * sizeof(double), s));
+  RCU(cudaMemsetAsync(acc, 0, size_t(2 * n_iter + 4) * sizeof(double), s));
 
   auto enqueue = [&](cudaStream_t q) -> cudaError_t {
     for (int32_t it = 0; it < n_iter; it++) {
       double* lli = want_ll ? ll + 2 * it : nullptr;
-      cudaError_t err = cudaMemsetAsync(acc, 0, sizeof(double), q);
+      cudaError_t err = cudaMemsetAsync(acc, 0, 3 * sizeof(double), q);
       if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it)], q);
       if (csc) {
         if (err == cudaSuccess)
-          err = half ? launch_mlem_forward_half(m, d_row_ptr, d_col, A.hval, A.rscale, d_y, d_x, rank, e, lli, q)
-                     : launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, rank, e, lli, q);
+          err = half ? launch_mlem_forward_half(m, d_row_ptr, d_col, A.hval, A.rscale, d_y, d_x, rank, e, lli, q,
+                                                next_row)
+                     : launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, rank, e, lli, q, next_row);
         if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 1)], q);
         if (err == cudaSuccess)
-          err = half ? launch_mlem_back_half(n, d_col_ptr, d_row_idx, A.htval, e, d_x, d_s, c, acc, true, q)
-                     : launch_mlem_back(n, d_col_ptr, d_row_idx, d_tval, e, d_x, d_s, c, acc, true, q);
+          err = half ? launch_mlem_back_half(n, d_col_ptr, d_row_idx, A.htval, e, d_x, d_s, c, acc, true, q, next_col)
+                     : launch_mlem_back(n, d_col_ptr, d_row_idx, d_tval, e, d_x, d_s, c, acc, true, q, next_col);
         if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 2)], q);
         if (err == cudaSuccess) err = launch_mlem_normalise_from(n, d_x, c, acc, q);
       } else {
@@ -1702,6 +1708,10 @@ raptr_status raptr_mlem_stream(raptr_ctx* ctx, const int32_t* d_cnl, int64_t n_l
     const int H = sm_level_capacity(level);
     int64_t per = std::max<int64_t>(1, int64_t(kStagingBudget / (size_t(H) * 8)));
     per = std::min<int64_t>(per, 65536);
+    // fewer rows per chunk when the device (or the library's memory limit)
+    // has less room than the usual staging
+    const size_t room = dev_available(ctx->device) + ctx->scratch_bytes;
+    per = std::max<int64_t>(1, std::min<int64_t>(per, int64_t(double(room) * 0.8 / (double(H) * 8 + 8))));
     RCHECK(ctx->ensure_scratch(Carve::need({size_t(per) * H * sizeof(int32_t), size_t(per) * H * sizeof(float),
                                             size_t(per) * sizeof(int32_t)})));
     Carve cv(ctx->d_scratch);
@@ -1914,11 +1924,11 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
   trace("reco_host: sensitivity");
   raptr_stream_stats sst{};
   if (streamed) {
-    // what the device holds now, less the row staging and working vectors
-    size_t free_b = 0, total_b = 0;
-    RSTEP(cudaMemGetInfo(&free_b, &total_b));
-    const int64_t reserve = (int64_t(3) << 30) + N * 24;
-    const int64_t resident = std::max<int64_t>(0, (int64_t(free_b) - reserve) * 9 / 10);
+    // what the library may still allocate, less the row staging (up to
+    // 1 GiB, less when the room is small) and the working vectors
+    const int64_t avail = int64_t(dev_available(device));
+    const int64_t reserve = std::min<int64_t>(int64_t(1) << 30, avail / 2) + N * 24 + (int64_t(64) << 20);
+    const int64_t resident = std::max<int64_t>(0, (avail - reserve) * 9 / 10);
     st = raptr_mlem_stream(ctx, d_list, M, nrays, seed, d_y, h_sens ? d_s : nullptr, nullptr, d_x, n_iter, resident,
                            &sst, s);
   } else {

@@ -15,9 +15,18 @@
 // are released and the allocation is retried once.  raptr_trim_memory()
 // releases them on request (before a caller allocates much memory by other
 // means, say).
+//
+// The environment variable RAPTR_DEVICE_MEMORY_LIMIT (bytes, read once)
+// caps what the library holds on a device (blocks in use and parked): an
+// allocation beyond it fails like one the device cannot satisfy, so that a
+// process sharing the device can keep the rest, and the callers that fall
+// back on a smaller working set (raptr_reco_host rebuilding rows in every
+// iteration) do so within the cap.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <unordered_map>
@@ -37,6 +46,8 @@ struct Block {
 
 std::mutex g_mu;
 std::unordered_map<void*, Block> g_live;                 // large blocks handed out
+std::unordered_map<void*, Block> g_small;                // smaller blocks handed out (counted only)
+std::map<int, size_t> g_in_use;                          // device -> bytes handed out
 std::map<int, std::multimap<size_t, void*>> g_parked;    // device -> size -> block
 std::map<int, size_t> g_parked_bytes;
 std::map<int, size_t> g_total;                           // device -> memory size
@@ -55,14 +66,59 @@ void release_locked(int device) {
   if (cur >= 0) cudaSetDevice(cur);
 }
 
+size_t memory_limit() {
+  static const size_t lim = [] {
+    const char* v = std::getenv("RAPTR_DEVICE_MEMORY_LIMIT");
+    return v ? size_t(std::strtoull(v, nullptr, 10)) : size_t(0);
+  }();
+  return lim;
+}
+
+// Whether `bytes` more may be handed out on `device` under the limit
+// (parked blocks released first when they are what stands in the way).
+// Holds g_mu.
+bool within_limit_locked(int device, size_t bytes) {
+  const size_t lim = memory_limit();
+  if (lim == 0) return true;
+  if (g_in_use[device] + g_parked_bytes[device] + bytes <= lim) return true;
+  release_locked(device);
+  return g_in_use[device] + bytes <= lim;
+}
+
 }  // namespace
+
+size_t dev_available(int device) {
+  size_t free_b = 0, total_b = 0;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != device) cudaSetDevice(device);
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    (void)cudaGetLastError();
+    free_b = 0;
+  }
+  if (cur >= 0 && cur != device) cudaSetDevice(cur);
+  std::lock_guard<std::mutex> lock(g_mu);
+  size_t avail = free_b + g_parked_bytes[device];  // parked blocks can be given back
+  const size_t lim = memory_limit();
+  if (lim > 0) avail = std::min(avail, lim > g_in_use[device] ? lim - g_in_use[device] : size_t(0));
+  return avail;
+}
 
 cudaError_t dev_alloc(void** p, size_t bytes) {
   *p = nullptr;
-  if (bytes < kMinCached) return cudaMalloc(p, bytes);
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  if (bytes < kMinCached) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!within_limit_locked(dev, bytes)) return cudaErrorMemoryAllocation;
+    e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) {
+      g_small[*p] = Block{bytes, dev};
+      g_in_use[dev] += bytes;
+    }
+    return e;
+  }
   std::lock_guard<std::mutex> lock(g_mu);
   auto& parked = g_parked[dev];
   auto it = parked.lower_bound(bytes);
@@ -70,9 +126,11 @@ cudaError_t dev_alloc(void** p, size_t bytes) {
     *p = it->second;
     g_live[*p] = Block{it->first, dev};
     g_parked_bytes[dev] -= it->first;
+    g_in_use[dev] += it->first;
     parked.erase(it);
     return cudaSuccess;
   }
+  if (!within_limit_locked(dev, bytes)) return cudaErrorMemoryAllocation;
   e = cudaMalloc(p, bytes);
   if (e == cudaErrorMemoryAllocation && !parked.empty()) {
     (void)cudaGetLastError();
@@ -84,6 +142,7 @@ cudaError_t dev_alloc(void** p, size_t bytes) {
     return e;
   }
   g_live[*p] = Block{bytes, dev};
+  g_in_use[dev] += bytes;
   return cudaSuccess;
 }
 
@@ -96,6 +155,13 @@ void dev_free(void* p) {
     if (it != g_live.end()) {
       b = it->second;
       g_live.erase(it);
+      g_in_use[b.device] -= b.bytes;
+    } else {
+      auto si = g_small.find(p);
+      if (si != g_small.end()) {
+        g_in_use[si->second.device] -= si->second.bytes;
+        g_small.erase(si);
+      }
     }
   }
   if (b.bytes == 0) {

@@ -24,6 +24,10 @@ long long launches_so_far();
 cudaError_t dev_alloc(void** p, size_t bytes);
 void dev_free(void* p);
 void dev_release(int device);
+// Bytes the library may still allocate on `device`: the device's free
+// memory plus the library's parked blocks, within RAPTR_DEVICE_MEMORY_LIMIT
+// when that is set.
+size_t dev_available(int device);
 template <class T>
 cudaError_t dev_malloc(T** p, size_t bytes) {
   void* q = nullptr;
@@ -156,11 +160,11 @@ cudaError_t launch_sens_half(int64_t n, const int64_t* cp, const int32_t* trow, 
 // e[rank_i] = rscale_i * y_i / (A x)_i (0 where y_i == 0).
 cudaError_t launch_mlem_forward_half(int64_t m, const int64_t* rp, const int32_t* col, const uint16_t* hval,
                                      const float* rscale, const float* y, const float* x, const int32_t* rank,
-                                     float* e, double* d_ll, cudaStream_t s);
-// c_j = sum h_kj e_k, compensated; with update as launch_mlem_back.
+                                     float* e, double* d_ll, cudaStream_t s, unsigned long long* next = nullptr);
+// c_j = sum h_kj e_k, compensated; with update and `next` as launch_mlem_back.
 cudaError_t launch_mlem_back_half(int64_t n, const int64_t* cp, const int32_t* trow, const uint16_t* htval,
                                   const float* e, const float* x, const float* sens, float* out, double* d_acc,
-                                  bool update, cudaStream_t s);
+                                  bool update, cudaStream_t s, unsigned long long* next = nullptr);
 // One MLEM iteration with FP64 vectors (x, e, xx: n / m / n doubles, acc one
 // double); s64 is the normalised sensitivity.
 cudaError_t launch_mlem_f64_iteration(int64_t m, int64_t n, const int64_t* rp, const int32_t* col, const float* val,
@@ -252,12 +256,17 @@ cudaError_t launch_transpose_blocked(int64_t m, int64_t n, int B, const int64_t*
                                      int64_t* colcount, int64_t* scan_tmp, int32_t* bad, int64_t* cp, int32_t* trow,
                                      float* tval, cudaStream_t s);
 // e_i = y_i / (A x)_i (0 for y_i == 0); optional FP64 log-likelihood sums.
+// With `next` (an 8-byte counter, zero at launch) the warps draw rows from
+// it, kRowChunk at a time.
 cudaError_t launch_mlem_forward(int64_t m, const int64_t* rp, const int32_t* col, const float* val, const float* y,
-                                const float* x, const int32_t* rank, float* e, double* d_ll, cudaStream_t s);
+                                const float* x, const int32_t* rank, float* e, double* d_ll, cudaStream_t s,
+                                unsigned long long* next = nullptr);
 // c_j = (A^T e)_j by columns; with update: out = x*c/(s+(s==0)), d_acc += sum.
+// With `next` (an 8-byte counter, zero at launch) the warps draw columns
+// from it instead of taking them by a grid stride.
 cudaError_t launch_mlem_back(int64_t n, const int64_t* cp, const int32_t* trow, const float* tval, const float* e,
                              const float* x, const float* sens, float* out, double* d_acc, bool update,
-                             cudaStream_t s);
+                             cudaStream_t s, unsigned long long* next = nullptr);
 cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s);
 cudaError_t launch_narrow_i64(const int64_t* in, int64_t n, int32_t* out, cudaStream_t s);
 cudaError_t launch_widen_i32(const int32_t* in, int64_t n, int64_t* out, cudaStream_t s);

@@ -162,11 +162,14 @@ __device__ __forceinline__ float row_dot_half(const int32_t* __restrict__ col, c
 __global__ void __launch_bounds__(kThreads) mlem_forward_half_kernel(
     int64_t m, const int64_t* __restrict__ rp, const int32_t* __restrict__ col, const uint16_t* __restrict__ hval,
     const float* __restrict__ rscale, const float* __restrict__ y, const float* __restrict__ x,
-    const int32_t* __restrict__ rank, float* __restrict__ e, double* __restrict__ ll) {
+    const int32_t* __restrict__ rank, float* __restrict__ e, double* __restrict__ ll, unsigned long long* next) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
   double ly = 0.0, lt = 0.0;
-  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+  // rows drawn kRowChunk at a time from `next` when given, as the FP32 pass
+  int64_t r0 = next ? warp_next(next, lane) * kRowChunk : (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  for (; r0 < m; r0 = next ? warp_next(next, lane) * kRowChunk : r0 + nw)
+  for (int64_t r = r0, r1 = next ? min(r0 + kRowChunk, m) : r0 + 1; r < r1; r++) {
     const float yi = __ldg(y + r);
     const int64_t dst = rank ? int64_t(__ldg(rank + r)) : r;
     if (yi == 0.f) {
@@ -193,6 +196,8 @@ __global__ void __launch_bounds__(kThreads) mlem_forward_half_kernel(
 // Column dot with binary16 values and compensated accumulation; lane q
 // takes quads q, q+32, ... (four consecutive entries: 16-byte index load,
 // 8-byte value load), each quad summed in FP32 and added with a two-sum.
+// Four quads per lane are loaded and gathered together (3-4 % faster than
+// two on the 70^3 x 5.14M matrix).
 __device__ __forceinline__ float col_dot_half(const int32_t* __restrict__ trow, const uint16_t* __restrict__ hv,
                                               int64_t b, int64_t e, const float* __restrict__ ev, int lane) {
   float s = 0.f, c = 0.f;
@@ -203,6 +208,26 @@ __device__ __forceinline__ float col_dot_half(const int32_t* __restrict__ trow, 
   const int4* t4 = reinterpret_cast<const int4*>(trow + a);
   const uint2* h4 = reinterpret_cast<const uint2*>(hv + a);
   int64_t q = lane;
+  for (; q + 96 < nq; q += 128) {
+    const int4 r0 = __ldcs(t4 + q), r1 = __ldcs(t4 + q + 32), r2 = __ldcs(t4 + q + 64), r3 = __ldcs(t4 + q + 96);
+    const uint2 w0 = __ldcs(h4 + q), w1 = __ldcs(h4 + q + 32), w2 = __ldcs(h4 + q + 64), w3 = __ldcs(h4 + q + 96);
+    const float g0 = __ldg(ev + r0.x), g1 = __ldg(ev + r0.y), g2 = __ldg(ev + r0.z), g3 = __ldg(ev + r0.w);
+    const float g4 = __ldg(ev + r1.x), g5 = __ldg(ev + r1.y), g6 = __ldg(ev + r1.z), g7 = __ldg(ev + r1.w);
+    const float g8 = __ldg(ev + r2.x), g9 = __ldg(ev + r2.y), g10 = __ldg(ev + r2.z), g11 = __ldg(ev + r2.w);
+    const float g12 = __ldg(ev + r3.x), g13 = __ldg(ev + r3.y), g14 = __ldg(ev + r3.z), g15 = __ldg(ev + r3.w);
+    const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&w0.x));
+    const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&w0.y));
+    const float2 f2 = __half22float2(*reinterpret_cast<const __half2*>(&w1.x));
+    const float2 f3 = __half22float2(*reinterpret_cast<const __half2*>(&w1.y));
+    const float2 f4 = __half22float2(*reinterpret_cast<const __half2*>(&w2.x));
+    const float2 f5 = __half22float2(*reinterpret_cast<const __half2*>(&w2.y));
+    const float2 f6 = __half22float2(*reinterpret_cast<const __half2*>(&w3.x));
+    const float2 f7 = __half22float2(*reinterpret_cast<const __half2*>(&w3.y));
+    two_sum_add(s, c, (f0.x * g0 + f0.y * g1) + (f1.x * g2 + f1.y * g3));
+    two_sum_add(s, c, (f2.x * g4 + f2.y * g5) + (f3.x * g6 + f3.y * g7));
+    two_sum_add(s, c, (f4.x * g8 + f4.y * g9) + (f5.x * g10 + f5.y * g11));
+    two_sum_add(s, c, (f6.x * g12 + f6.y * g13) + (f7.x * g14 + f7.y * g15));
+  }
   for (; q + 32 < nq; q += 64) {
     const int4 r0 = __ldcs(t4 + q), r1 = __ldcs(t4 + q + 32);
     const uint2 w0 = __ldcs(h4 + q), w1 = __ldcs(h4 + q + 32);
@@ -236,6 +261,8 @@ __device__ __forceinline__ float col_dot_half(const int32_t* __restrict__ trow, 
   return s + c;
 }
 
+// Columns are drawn from the counter at `next` when it is given (see
+// mlem_back_kernel), else taken by a grid stride.
 template <bool UPDATE>
 __global__ void __launch_bounds__(kThreads) mlem_back_half_kernel(int64_t n, const int64_t* __restrict__ cp,
                                                                   const int32_t* __restrict__ trow,
@@ -243,11 +270,13 @@ __global__ void __launch_bounds__(kThreads) mlem_back_half_kernel(int64_t n, con
                                                                   const float* __restrict__ e,
                                                                   const float* __restrict__ x,
                                                                   const float* __restrict__ sens,
-                                                                  float* __restrict__ out, double* __restrict__ acc) {
+                                                                  float* __restrict__ out, double* __restrict__ acc,
+                                                                  unsigned long long* next) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
   double sum = 0.0;
-  for (int64_t j = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; j < n; j += nw) {
+  int64_t j = next ? warp_next(next, lane) : (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  for (; j < n; j = next ? warp_next(next, lane) : j + nw) {
     const float c = col_dot_half(trow, htval, cp[j], cp[j + 1], e, lane);
     if (lane == 0) {
       if (UPDATE) {
@@ -373,21 +402,21 @@ cudaError_t launch_sens_half(int64_t n, const int64_t* cp, const int32_t* trow, 
 
 cudaError_t launch_mlem_forward_half(int64_t m, const int64_t* rp, const int32_t* col, const uint16_t* hval,
                                      const float* rscale, const float* y, const float* x, const int32_t* rank,
-                                     float* e, double* d_ll, cudaStream_t s) {
+                                     float* e, double* d_ll, cudaStream_t s, unsigned long long* next) {
   if (m <= 0) return cudaSuccess;
-  mlem_forward_half_kernel<<<grid_rows(m), kThreads, 0, s>>>(m, rp, col, hval, rscale, y, x, rank, e, d_ll);
+  mlem_forward_half_kernel<<<grid_rows(m), kThreads, 0, s>>>(m, rp, col, hval, rscale, y, x, rank, e, d_ll, next);
   note_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mlem_back_half(int64_t n, const int64_t* cp, const int32_t* trow, const uint16_t* htval,
                                   const float* e, const float* x, const float* sens, float* out, double* d_acc,
-                                  bool update, cudaStream_t s) {
+                                  bool update, cudaStream_t s, unsigned long long* next) {
   if (n <= 0) return cudaSuccess;
   if (update)
-    mlem_back_half_kernel<true><<<grid_rows(n), kThreads, 0, s>>>(n, cp, trow, htval, e, x, sens, out, d_acc);
+    mlem_back_half_kernel<true><<<grid_rows(n), kThreads, 0, s>>>(n, cp, trow, htval, e, x, sens, out, d_acc, next);
   else
-    mlem_back_half_kernel<false><<<grid_rows(n), kThreads, 0, s>>>(n, cp, trow, htval, e, x, sens, out, d_acc);
+    mlem_back_half_kernel<false><<<grid_rows(n), kThreads, 0, s>>>(n, cp, trow, htval, e, x, sens, out, d_acc, next);
   note_launches(1);
   return cudaGetLastError();
 }

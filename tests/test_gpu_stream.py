@@ -98,3 +98,36 @@ def test_stream_rejects_bad_arguments(rlib, torch, case):
     bad[7] = ctx.n_channels  # out of range
     with pytest.raises(RuntimeError):
         ctx.mlem_stream(bad, 100, SEED, y, s, x, 2, 0)
+
+
+def test_reco_host_falls_back_to_rebuilding_rows(rlib, torch, tmp_path):
+    """raptr_reco_host in a process whose library memory is capped
+    (RAPTR_DEVICE_MEMORY_LIMIT, 600 MB) below what the build, the matrix
+    and its transpose need: the call keeps the rows that fit resident,
+    rebuilds the others in every iteration, and returns the image of the
+    uncapped call (1e-5; the back projections sum in another order)."""
+    import os
+    import subprocess
+    import sys
+
+    g = cfg.SMALL
+    rng = np.random.default_rng(17)
+    y = rng.poisson(3.0, g.n_channels).astype(np.float32)
+    np.save(tmp_path / "y.npy", y)
+    x_ref, st_ref = rlib.reco_host(g, y, 100, SEED, 6)
+    assert st_ref["streamed_rows"] == 0
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r)\n"
+        "import raptr_b200 as R\n"
+        "y = np.load(%r)\n"
+        "x, st = R.reco_host(R.SMALL, y, 100, %d, 6)\n"
+        "np.save(%r, x); print(st['streamed_rows'], st['nnz'])\n"
+    ) % (root, str(tmp_path / "y.npy"), SEED, str(tmp_path / "x.npy"))
+    env = dict(os.environ, RAPTR_DEVICE_MEMORY_LIMIT=str(600 << 20))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    streamed, resident_entries = (int(v) for v in r.stdout.split())
+    assert 0 < streamed < g.n_channels and 0 < resident_entries < st_ref["nnz"]
+    x = np.load(tmp_path / "x.npy")
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < RTOL
