@@ -54,8 +54,10 @@ MEAS_SEED = 20240
 # (dram__bytes_read.sum + dram__bytes_write.sum) / entries.  The roofline's `traffic` scales them by
 # the entries of the timed matrix (traffic grows with the entries).
 TRAFFIC_BYTES_PER_ENTRY = {
-    "mlem_back_kernel": (1.541829e9 + 5.229568e6) / 191091787,
-    "mlem_forward_kernel": (1.534958e9 + 5.378560e6) / 191091787,
+    # column-slab profile case (x slabs 33-36, full-length columns)
+    "mlem_back_kernel": (3.020836e9 + 5.886464e6) / 371438029,
+    # row profile case (rows 0..299,999, full rows)
+    "mlem_forward_kernel": (1.539569e9 + 4.874752e6) / 191091787,
 }
 
 
@@ -702,7 +704,7 @@ def main():
             out["roofline"] = {"bound": "hbm", "kernel": dom[0], "achieved": round(dom[1], 1), "peak": peak,
                                "unit": "GB/s", "frac": round(dom[1] / peak, 4), "peak_source": peak_kind,
                                "traffic": int(TRAFFIC_BYTES_PER_ENTRY[dom[0]] * nnz),
-                               "traffic_source": "ncu DRAM bytes per entry of the profile case x entries",
+                               "traffic_source": "ncu DRAM bytes per entry of the kernel's profile case x entries",
                                "algorithmic_bytes": int(dom[2]), "launch_ms": round(dom[3], 4)}
             out["roofline_all"] = {
                 "mlem_forward_kernel": {"achieved": round(r_f, 1), "frac": round(r_f / peak, 4),
@@ -715,12 +717,13 @@ def main():
 
     # End to end through the public C ABI from host buffers (rank 0, N=1).
     if not args.no_e2e and world == 1:
-        times, st = [], None
+        times, sts, st = [], [], None
         R.reco_host(g, y_full, w["nrays"], SEED, w["niter"], device=dev)  # warm-up, untimed
-        for _ in range(max(1, min(args.steps, 2))):
+        for _ in range(max(1, min(args.steps, 3))):
             t0 = time.perf_counter()
             x_h, st = R.reco_host(g, y_full, w["nrays"], SEED, w["niter"], device=dev)
             times.append(time.perf_counter() - t0)
+            sts.append(st)
         e2e_s = statistics.mean(times)
         out["e2e"] = {"value": w["niter"] / e2e_s, "unit": "MLEM iterations/s",
                       "h2d_bytes_per_step": int(st["h2d_bytes"]), "d2h_bytes_per_step": int(st["d2h_bytes"]),
@@ -728,6 +731,10 @@ def main():
                       "phases_ms": {k: round(st[k], 3) for k in ("setup_ms", "inputs_ms", "build_ms", "transpose_ms",
                                                                  "sens_ms", "iter_ms", "output_ms", "release_ms",
                                                                  "wall_ms")},
+                      "calls": [{"wall_s": round(t, 4),
+                                 **{k: round(c[k], 3) for k in ("build_ms", "transpose_ms", "sens_ms", "iter_ms",
+                                                                "release_ms", "wall_ms")}}
+                                for t, c in zip(times, sts)],
                       "streamed_rows": int(st["streamed_rows"])}
     if rank == 0 and world == 1 and not args.no_forms:
         peak, _ = measured_peaks()
