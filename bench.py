@@ -336,25 +336,28 @@ def run_job(R, torch, ctx, w, lst, y_dev, dist=None, keep=False):
 
 
 def precision_report(R, torch, ctx, w, lst, y_dev, peak):
-    """The FP16-matrix form beside the FP32 one, both against the FP64
-    iteration on the same matrix: relative L2 and max error of the image
-    after 10 / 25 / 50 iterations, iteration rates (CUDA graph) and the
-    roofline of the FP16 passes."""
+    """The FP16-matrix form (plain: 6 bytes per entry; delta-coded: 4) beside
+    the FP32 one, all against the FP64 iteration on the same matrix:
+    relative L2 and max error of the image after 10 / 25 / 50 iterations,
+    iteration rates (CUDA graph) and the roofline of the FP16 passes."""
     g = w["geom"]
     n = g.n_voxels
     A = ctx.build(lst, w["nrays"], SEED)
     A.transpose()
     A.to_half()
+    A.to_packed()
     nnz, m = A.nnz, A.m
+    pwords, twords = A.pword.numel(), A.tword.numel()
     s64, s32 = R.sensitivity(A)
     h64, h32 = R.sensitivity_half(A)
     marks = [c for c in (10, 25, 50) if c <= w["niter"]] or [w["niter"]]
     x64 = torch.full((n,), 1.0 / n, dtype=torch.float64, device="cuda")
     x32 = torch.full((n,), np.float32(1.0 / n), device="cuda")
     x16 = torch.full((n,), np.float32(1.0 / n), device="cuda")
+    xpk = torch.full((n,), np.float32(1.0 / n), device="cuda")
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    errs = {"fp32": {}, "fp16": {}}
-    ms = {"fp32": 0.0, "fp16": 0.0}
+    errs = {"fp32": {}, "fp16": {}, "fp16_delta": {}}
+    ms = {"fp32": 0.0, "fp16": 0.0, "fp16_delta": 0.0}
     kt16 = []
     done = 0
     for mark in marks:
@@ -365,11 +368,14 @@ def precision_report(R, torch, ctx, w, lst, y_dev, peak):
         ev[1].record()
         ctx.mlem_half(A, y_dev, h32, x16, k, use_graph=True)
         ev[2].record()
+        ctx.mlem_packed(A, y_dev, h32, xpk, k, use_graph=True)
+        ev[3].record()
         torch.cuda.synchronize()
         ms["fp32"] += ev[0].elapsed_time(ev[1])
         ms["fp16"] += ev[1].elapsed_time(ev[2])
+        ms["fp16_delta"] += ev[2].elapsed_time(ev[3])
         ref = x64
-        for name, x in (("fp32", x32), ("fp16", x16)):
+        for name, x in (("fp32", x32), ("fp16", x16), ("fp16_delta", xpk)):
             d = x.double() - ref
             errs[name][str(mark)] = {"rel_l2": float(d.norm() / ref.norm()),
                                      "max_rel": float(d.abs().max() / ref.abs().max())}
@@ -379,17 +385,28 @@ def precision_report(R, torch, ctx, w, lst, y_dev, peak):
     fwd_ms, back_ms = float(kt16[:, 0].mean()), float(kt16[:, 1].mean())
     fwd_b = nnz * 6 + (m + 1) * 8 + m * 4 * 4 + n * 4
     back_b = nnz * 6 + (n + 1) * 8 + 3 * n * 4 + m * 4
+    ktp = ctx.mlem_packed(A, y_dev, h32, xpk.clone(), 5, use_graph=False, kernel_times=True)
+    pf_ms, pb_ms = float(ktp[:, 0].mean()), float(ktp[:, 1].mean())
+    # words (4 bytes per entry, plus the steps above 65535 and the padding),
+    # quad offsets and anchors, then the vectors as for the plain form
+    pf_b = pwords * 4 + (m + 1) * 8 + m * 4 + m * 4 * 4 + n * 4
+    pb_b = twords * 4 + (n + 1) * 8 + n * 4 + 3 * n * 4 + m * 4
+
+    def line(b, t):
+        return {"achieved": round(b / t / 1e6, 1), "frac": round(b / t / 1e6 / peak, 4), "ms": round(t, 4)}
+
     out = {
         "iterations": done,
         "iters_per_s": {k: done / (v / 1e3) for k, v in ms.items()},
         "speedup_fp16_vs_fp32": ms["fp32"] / ms["fp16"],
+        "speedup_fp16_delta_vs_fp32": ms["fp32"] / ms["fp16_delta"],
         "error_vs_fp64": errs,
-        "matrix_bytes_per_entry": {"fp32": 8, "fp16": 6},
+        "matrix_bytes_per_entry": {"fp32": 8, "fp16": 6, "fp16_delta": round(4 * (pwords + twords) / (2 * nnz), 4)},
         "roofline_fp16": {
-            "mlem_forward_half_kernel": {"achieved": round(fwd_b / fwd_ms / 1e6, 1),
-                                         "frac": round(fwd_b / fwd_ms / 1e6 / peak, 4), "ms": round(fwd_ms, 4)},
-            "mlem_back_half_kernel": {"achieved": round(back_b / back_ms / 1e6, 1),
-                                      "frac": round(back_b / back_ms / 1e6 / peak, 4), "ms": round(back_ms, 4)},
+            "mlem_forward_half_kernel": line(fwd_b, fwd_ms),
+            "mlem_back_half_kernel": line(back_b, back_ms),
+            "mlem_forward_packed_kernel": line(pf_b, pf_ms),
+            "mlem_back_packed_kernel": line(pb_b, pb_ms),
         },
         "reference": "FP64 vectors and accumulation over the FP32 matrix (raptr_mlem_f64, GPU)",
     }

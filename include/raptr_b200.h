@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define RAPTR_ABI_VERSION 4
+#define RAPTR_ABI_VERSION 5
 
 typedef enum raptr_status {
   RAPTR_OK = 0,
@@ -313,6 +313,38 @@ raptr_status raptr_mlem_half(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t
                              const uint16_t* d_hval, const float* d_rscale, const int64_t* d_col_ptr,
                              const int32_t* d_row_idx, const uint16_t* d_htval, const float* d_y, const float* d_s,
                              float* d_x, int32_t n_iter, const raptr_mlem_opts* opts, void* stream);
+/* Delta-coded FP16 runs, 4 bytes per entry instead of 6: each of the count
+ * runs of (d_ptr, d_idx, d_hv) -- the rows of a CSR with its binary16
+ * values, or the columns of its transpose -- as 32-bit words (h << 16) | d,
+ * d the run's index step from the previous word (from the run's anchor,
+ * its first index, for the first word).  A step above 65535 takes extra
+ * words of step 65535 and value 0 before the entry's word.  Run r holds
+ * the words [4*d_seg[r], 4*d_seg[r+1]) (offsets in quads of four words; a
+ * run's last quad is padded with words 0); d_anchor[r] is its first index
+ * (0 for an empty run).  Indices must ascend within a run.
+ * Two phases: with d_words null, fills d_seg (count + 1 int64) and
+ * *h_words (the words needed); then, with d_words (16-byte aligned,
+ * words_cap >= *h_words) and d_anchor (count int32), the runs.
+ * Synchronises. */
+raptr_status raptr_pack_half(int64_t count, const int64_t* d_ptr, const int32_t* d_idx, const uint16_t* d_hv,
+                             int64_t* d_seg, int32_t* d_anchor, uint32_t* d_words, int64_t words_cap,
+                             int64_t* h_words, void* stream);
+/* The matrix's FP16 form delta-coded (raptr_pack_half of its CSR and of its
+ * transpose, kept with the matrix); requires raptr_matrix_half.  Synchronises. */
+raptr_status raptr_matrix_packed(raptr_matrix* A, void* stream);
+raptr_status raptr_matrix_packed_info(const raptr_matrix* A, int64_t** d_seg, int32_t** d_anchor,
+                                      uint32_t** d_words, int64_t** d_tseg, int32_t** d_tanchor,
+                                      uint32_t** d_twords);
+/* raptr_mlem_half over the delta-coded runs: rows (d_seg, d_anchor,
+ * d_words) with the row scales d_rscale, columns of the transpose (d_tseg,
+ * d_tanchor, d_twords) in the order opts->d_row_rank gives (as for
+ * raptr_mlem_half).  The same values and accumulation as raptr_mlem_half;
+ * per entry 4 matrix bytes per pass instead of 6. */
+raptr_status raptr_mlem_packed(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_seg, const int32_t* d_anchor,
+                               const uint32_t* d_words, const float* d_rscale, const int64_t* d_tseg,
+                               const int32_t* d_tanchor, const uint32_t* d_twords, const float* d_y,
+                               const float* d_s, float* d_x, int32_t n_iter, const raptr_mlem_opts* opts,
+                               void* stream);
 /* The same iteration with FP64 vectors and accumulation over the FP32
  * matrix (the reference for the FP32 and FP16 images): d_s64 is the
  * normalised sensitivity, d_x64 the image (updated in place); h_loglik,

@@ -153,6 +153,11 @@ _SIGNATURES = {
     "raptr_sensitivity_half": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, VP]),
     "raptr_mlem_half": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32,
                                   C.POINTER(raptr_mlem_opts), VP]),
+    "raptr_pack_half": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, I64, C.POINTER(I64), VP]),
+    "raptr_matrix_packed": (C.c_int, [VP, VP]),
+    "raptr_matrix_packed_info": (C.c_int, [VP] + [C.POINTER(VP)] * 6),
+    "raptr_mlem_packed": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32,
+                                    C.POINTER(raptr_mlem_opts), VP]),
     "raptr_mlem_f64": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32, VP, VP]),
     "raptr_mlem_batch": (C.c_int, [VP, I64, I64, I32, I32, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32, I32,
                                    C.POINTER(raptr_mlem_opts), VP]),
@@ -322,6 +327,35 @@ class Matrix:
         self.pscale = torch.as_tensor(_DeviceArray(ps.value, (mm,), "<f4", own), device=dev)[:self.m]
         return self
 
+    # delta-coded FP16 form (to_packed): rows and transpose columns as runs
+    # of words (h << 16) | index step
+    pseg = None
+    panchor = None
+    pword = None
+    tseg = None
+    tanchor = None
+    tword = None
+
+    def to_packed(self, stream=None) -> "Matrix":
+        """Builds the delta-coded copy of the FP16 form (raptr_matrix_packed);
+        builds the FP16 form first if needed."""
+        if self.hval is None:
+            self.to_half(stream)
+        _check(lib().raptr_matrix_packed(self._h, _stream(stream)))
+        p = [VP() for _ in range(6)]
+        _check(lib().raptr_matrix_packed_info(self._h, *[C.byref(v) for v in p]))
+        torch = _torch()
+        dev = torch.device("cuda", self.device)
+        own = self._owner
+        self.pseg = torch.as_tensor(_DeviceArray(p[0].value, (self.m + 1,), "<i8", own), device=dev)
+        self.tseg = torch.as_tensor(_DeviceArray(p[3].value, (self.n + 1,), "<i8", own), device=dev)
+        nw, ntw = packed_words(self.pseg, self.m), packed_words(self.tseg, self.n)
+        self.panchor = torch.as_tensor(_DeviceArray(p[1].value, (max(self.m, 1),), "<i4", own), device=dev)
+        self.pword = torch.as_tensor(_DeviceArray(p[2].value, (max(nw, 4),), "<i4", own), device=dev)[:nw]
+        self.tanchor = torch.as_tensor(_DeviceArray(p[4].value, (max(self.n, 1),), "<i4", own), device=dev)
+        self.tword = torch.as_tensor(_DeviceArray(p[5].value, (max(ntw, 4),), "<i4", own), device=dev)[:ntw]
+        return self
+
     def to_numpy(self):
         return self.row_ptr.cpu().numpy(), self.col.cpu().numpy(), self.val.cpu().numpy()
 
@@ -466,6 +500,25 @@ class Context:
             out.append(np.array(kt[:2 * niter], np.float64).reshape(niter, 2))
         return None if not out else (out[0] if len(out) == 1 else tuple(out))
 
+    def mlem_packed(self, A: Matrix, y, s, x, niter: int, use_graph: bool = True, loglik: bool = False,
+                    kernel_times: bool = False, stream=None):
+        """MLEM iterations with A's delta-coded FP16 copy (A.to_packed()); as
+        mlem_half()."""
+        assert A.pword is not None, "call A.to_packed() first"
+        ll = (C.c_double * max(niter, 1))() if loglik else None
+        kt = (C.c_float * max(2 * niter, 1))() if kernel_times else None
+        opts = raptr_mlem_opts(1 if use_graph else 0, C.cast(ll, C.POINTER(C.c_double)) if loglik else None,
+                               C.cast(kt, C.POINTER(C.c_float)) if kernel_times else None, _ptr(A.row_rank))
+        _check(lib().raptr_mlem_packed(self._h, A.m, A.n, _ptr(A.pseg), _ptr(A.panchor), _ptr(A.pword),
+                                       _ptr(A.rscale), _ptr(A.tseg), _ptr(A.tanchor), _ptr(A.tword), _ptr(y),
+                                       _ptr(s), _ptr(x), niter, C.byref(opts), _stream(stream)))
+        out = []
+        if loglik:
+            out.append(np.array(ll[:niter]))
+        if kernel_times:
+            out.append(np.array(kt[:2 * niter], np.float64).reshape(niter, 2))
+        return None if not out else (out[0] if len(out) == 1 else tuple(out))
+
     def _batch_arrays(self, A: Matrix, half: bool):
         if not A.has_transpose:
             A.transpose()
@@ -560,6 +613,28 @@ class Server:
 
 
 # -- context-free operations ---------------------------------------------------
+
+
+def packed_words(seg, count: int) -> int:
+    """Words of delta-coded runs whose quad offsets are seg (count + 1)."""
+    return int(seg[count].item()) * 4
+
+
+def pack_half(ptr, idx, hv, stream=None):
+    """Delta-coded FP16 runs of (ptr, idx, hv) (raptr_pack_half): returns
+    (seg, anchor, words) as device tensors (words as int32 bit patterns)."""
+    torch = _torch()
+    count = ptr.numel() - 1
+    dev = ptr.device
+    seg = torch.empty(count + 1, dtype=torch.int64, device=dev)
+    anchor = torch.empty(max(count, 1), dtype=torch.int32, device=dev)
+    nw = I64()
+    _check(lib().raptr_pack_half(count, _ptr(ptr), _ptr(idx), _ptr(hv), _ptr(seg), _ptr(anchor), None, 0,
+                                 C.byref(nw), _stream(stream)))
+    words = torch.empty(max(nw.value, 4), dtype=torch.int32, device=dev)
+    _check(lib().raptr_pack_half(count, _ptr(ptr), _ptr(idx), _ptr(hv), _ptr(seg), _ptr(anchor), _ptr(words),
+                                 words.numel(), C.byref(nw), _stream(stream)))
+    return seg, anchor[:count], words[:nw.value]
 
 
 def sensitivity_half(A: Matrix, stream=None):
@@ -702,7 +777,7 @@ def reco_host(geom: Geometry, y: np.ndarray, nrays: int, seed: int, niter: int, 
 
 
 __all__ = [
-    "Geometry", "SMALL", "FULL", "FINE", "WORKLOADS", "epet_geometry", "phantom", "poisson_measurement", "Context",
+    "pack_half", "packed_words", "Geometry", "SMALL", "FULL", "FINE", "WORKLOADS", "epet_geometry", "phantom", "poisson_measurement", "Context",
     "Matrix", "spmv", "sensitivity", "mlem_project", "mlem_forward", "mlem_back", "csr_transpose", "mlem_update", "divides", "divides_multiplies", "scales",
     "vsum", "coo2csr", "csr2ecsr", "reco_host", "lib", "RaptrError", "OP_N", "OP_T", "trim_memory",
 ]

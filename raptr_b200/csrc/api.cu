@@ -250,6 +250,15 @@ struct raptr_matrix {
   float* pscale = nullptr;   // rscale by position of the transpose
   uint16_t* hval = nullptr;  // CSR order
   uint16_t* htval = nullptr; // transpose order
+  // the FP16 form delta-coded (raptr_pack_half of the CSR and of the
+  // transpose), built on request
+  int64_t* pseg = nullptr;
+  int32_t* panchor = nullptr;
+  uint32_t* pword = nullptr;
+  int64_t* tseg = nullptr;
+  int32_t* tanchor = nullptr;
+  uint32_t* tword = nullptr;
+  int64_t pwords = 0, twords = 0;
 };
 
 namespace {
@@ -834,6 +843,12 @@ raptr_status raptr_matrix_destroy(raptr_matrix* A) {
   dev_free(A->pscale);
   dev_free(A->hval);
   dev_free(A->htval);
+  dev_free(A->pseg);
+  dev_free(A->panchor);
+  dev_free(A->pword);
+  dev_free(A->tseg);
+  dev_free(A->tanchor);
+  dev_free(A->tword);
   if (trace_on()) trace("matrix released: %.2f ms", trace_ms() - t0);
   delete A;
   return RAPTR_OK;
@@ -1194,6 +1209,13 @@ struct MlemArrays {
   const int32_t* trow = nullptr;
   const float* tval = nullptr;
   const uint16_t* htval = nullptr;
+  // delta-coded FP16 runs (with rscale): rows and transpose columns
+  const int64_t* pseg = nullptr;
+  const int32_t* panchor = nullptr;
+  const uint32_t* pword = nullptr;
+  const int64_t* tseg = nullptr;
+  const int32_t* tanchor = nullptr;
+  const uint32_t* tword = nullptr;
 };
 
 raptr_status mlem_impl(raptr_ctx* ctx, int64_t m, int64_t n, const MlemArrays& A, const float* d_y, const float* d_s,
@@ -1204,13 +1226,14 @@ raptr_status mlem_impl(raptr_ctx* ctx, int64_t m, int64_t n, const MlemArrays& A
   const int64_t* d_col_ptr = A.cp;
   const int32_t* d_row_idx = A.trow;
   const float* d_tval = A.tval;
+  const bool packed = A.pword != nullptr;
   const bool half = A.htval != nullptr;
   if (n_iter == 0) return RAPTR_OK;
   DeviceScope ds(ctx->device);
   const bool want_ll = opts && opts->h_loglik;
   const bool want_times = opts && opts->h_kernel_ms;
   const bool use_graph = opts && opts->use_graph && !want_times;
-  const bool csc = d_col_ptr != nullptr;
+  const bool csc = d_col_ptr != nullptr || packed;
   const int32_t* rank = opts ? opts->d_row_rank : nullptr;
   std::vector<cudaEvent_t> evs;
   if (want_times) {
@@ -1239,13 +1262,17 @@ raptr_status mlem_impl(raptr_ctx* ctx, int64_t m, int64_t n, const MlemArrays& A
       if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it)], q);
       if (csc) {
         if (err == cudaSuccess)
-          err = half ? launch_mlem_forward_half(m, d_row_ptr, d_col, A.hval, A.rscale, d_y, d_x, rank, e, lli, q,
-                                                next_row)
-                     : launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, rank, e, lli, q, next_row);
+          err = packed ? launch_mlem_forward_packed(m, A.pseg, A.panchor, A.pword, A.rscale, d_y, d_x, rank, e, lli,
+                                                    next_row, q)
+                : half ? launch_mlem_forward_half(m, d_row_ptr, d_col, A.hval, A.rscale, d_y, d_x, rank, e, lli, q,
+                                                  next_row)
+                       : launch_mlem_forward(m, d_row_ptr, d_col, d_val, d_y, d_x, rank, e, lli, q, next_row);
         if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 1)], q);
         if (err == cudaSuccess)
-          err = half ? launch_mlem_back_half(n, d_col_ptr, d_row_idx, A.htval, e, d_x, d_s, c, acc, true, q, next_col)
-                     : launch_mlem_back(n, d_col_ptr, d_row_idx, d_tval, e, d_x, d_s, c, acc, true, q, next_col);
+          err = packed ? launch_mlem_back_packed(n, A.tseg, A.tanchor, A.tword, e, d_x, d_s, c, acc, true, next_col, q)
+                : half ? launch_mlem_back_half(n, d_col_ptr, d_row_idx, A.htval, e, d_x, d_s, c, acc, true, q,
+                                               next_col)
+                       : launch_mlem_back(n, d_col_ptr, d_row_idx, d_tval, e, d_x, d_s, c, acc, true, q, next_col);
         if (want_times && err == cudaSuccess) err = cudaEventRecord(evs[size_t(3 * it + 2)], q);
         if (err == cudaSuccess) err = launch_mlem_normalise_from(n, d_x, c, acc, q);
       } else {
@@ -1355,6 +1382,27 @@ raptr_status raptr_mlem_half(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t
   return mlem_impl(ctx, m, n, A, d_y, d_s, d_x, n_iter, opts, as_stream(stream));
 }
 
+raptr_status raptr_mlem_packed(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_seg, const int32_t* d_anchor,
+                               const uint32_t* d_words, const float* d_rscale, const int64_t* d_tseg,
+                               const int32_t* d_tanchor, const uint32_t* d_twords, const float* d_y,
+                               const float* d_s, float* d_x, int32_t n_iter, const raptr_mlem_opts* opts,
+                               void* stream) {
+  if (!ctx || m < 0 || n <= 0 || n_iter < 0 || !d_y || !d_s || !d_x || !d_tseg || !d_tanchor || !d_twords ||
+      (m > 0 && (!d_seg || !d_anchor || !d_words || !d_rscale)))
+    return fail(RAPTR_ERR_INVALID, "bad argument");
+  if (((reinterpret_cast<uintptr_t>(d_words) | reinterpret_cast<uintptr_t>(d_twords)) & 15u) != 0)
+    return fail(RAPTR_ERR_INVALID, "the words of the delta-coded runs must be 16-byte aligned");
+  MlemArrays A;
+  A.rscale = d_rscale;
+  A.pseg = d_seg;
+  A.panchor = d_anchor;
+  A.pword = d_words;
+  A.tseg = d_tseg;
+  A.tanchor = d_tanchor;
+  A.tword = d_twords;
+  return mlem_impl(ctx, m, n, A, d_y, d_s, d_x, n_iter, opts, as_stream(stream));
+}
+
 raptr_status raptr_mlem_f64(raptr_ctx* ctx, int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
                             const float* d_val, const int64_t* d_col_ptr, const int32_t* d_row_idx,
                             const float* d_tval, const int32_t* d_row_rank, const float* d_y, const double* d_s64,
@@ -1427,6 +1475,95 @@ raptr_status raptr_matrix_half_info(const raptr_matrix* A, uint16_t** d_hval, fl
   return RAPTR_OK;
 }
 
+raptr_status raptr_pack_half(int64_t count, const int64_t* d_ptr, const int32_t* d_idx, const uint16_t* d_hv,
+                             int64_t* d_seg, int32_t* d_anchor, uint32_t* d_words, int64_t words_cap,
+                             int64_t* h_words, void* stream) {
+  if (count < 0 || !d_ptr || !d_seg || !h_words) return fail(RAPTR_ERR_INVALID, "bad argument");
+  if (d_words && (!d_anchor || !d_idx || !d_hv)) return fail(RAPTR_ERR_INVALID, "bad argument");
+  if ((reinterpret_cast<uintptr_t>(d_words) & 15u) != 0) return fail(RAPTR_ERR_INVALID, "d_words is not 16-byte aligned");
+  cudaStream_t s = as_stream(stream);
+  int64_t *quads = nullptr, *tmp = nullptr;
+  int32_t* bad = nullptr;
+  int32_t h_bad = 0;
+  int64_t h_quads = 0;
+  cudaError_t e = cudaMallocAsync(&quads, size_t(std::max<int64_t>(count, 1)) * sizeof(int64_t), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&tmp, size_t(scan_temp_elems(count)) * sizeof(int64_t), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&bad, sizeof(int32_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
+  if (e == cudaSuccess) e = launch_pack_count(count, d_ptr, d_idx, quads, bad, s);
+  if (e == cudaSuccess) e = launch_scan_i64(quads, count, d_seg, tmp, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_quads, d_seg + count, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  const bool fill = e == cudaSuccess && !h_bad && d_words && h_quads * 4 <= words_cap;
+  if (fill) e = launch_pack_fill(count, d_ptr, d_idx, d_hv, d_seg, d_anchor, d_words, s);
+  if (fill && e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFreeAsync(quads, s);
+  cudaFreeAsync(tmp, s);
+  cudaFreeAsync(bad, s);
+  if (e != cudaSuccess) return cuda_fail(e, "raptr_pack_half");
+  if (h_bad) return fail(RAPTR_ERR_INVALID, "indices descend within a run");
+  *h_words = h_quads * 4;
+  if (d_words && h_quads * 4 > words_cap) return fail(RAPTR_ERR_INVALID, "words_cap is below the words needed");
+  return RAPTR_OK;
+}
+
+raptr_status raptr_matrix_packed(raptr_matrix* A, void* stream) {
+  if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
+  if (!A->hval) return fail(RAPTR_ERR_INVALID, "the delta-coded form needs the FP16 form: call raptr_matrix_half first");
+  if (A->pword) return RAPTR_OK;
+  DeviceScope ds(A->device);
+  raptr_status st = RAPTR_OK;
+  auto pack = [&](int64_t count, const int64_t* ptr, const int32_t* idx, const uint16_t* hv, int64_t** seg,
+                  int32_t** anc, uint32_t** words, int64_t* nwords) {
+    if (st != RAPTR_OK) return;
+    cudaError_t e = dev_malloc(seg, size_t(count + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = dev_malloc(anc, size_t(std::max<int64_t>(count, 1)) * sizeof(int32_t));
+    if (e != cudaSuccess) {
+      st = cuda_fail(e, "raptr_matrix_packed");
+      return;
+    }
+    st = raptr_pack_half(count, ptr, idx, hv, *seg, *anc, nullptr, 0, nwords, stream);
+    if (st != RAPTR_OK) return;
+    e = dev_malloc(words, size_t(std::max<int64_t>(*nwords, 4)) * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+      st = cuda_fail(e, "raptr_matrix_packed");
+      return;
+    }
+    st = raptr_pack_half(count, ptr, idx, hv, *seg, *anc, *words, *nwords, nwords, stream);
+  };
+  pack(A->m, A->rp, A->col, A->hval, &A->pseg, &A->panchor, &A->pword, &A->pwords);
+  pack(A->n, A->cp, A->trow, A->htval, &A->tseg, &A->tanchor, &A->tword, &A->twords);
+  if (st != RAPTR_OK) {
+    const std::string msg = g_last_error;
+    dev_free(A->pseg);
+    dev_free(A->panchor);
+    dev_free(A->pword);
+    dev_free(A->tseg);
+    dev_free(A->tanchor);
+    dev_free(A->tword);
+    A->pseg = A->tseg = nullptr;
+    A->panchor = A->tanchor = nullptr;
+    A->pword = A->tword = nullptr;
+    A->pwords = A->twords = 0;
+    return fail(st, msg);
+  }
+  return RAPTR_OK;
+}
+
+raptr_status raptr_matrix_packed_info(const raptr_matrix* A, int64_t** d_seg, int32_t** d_anchor,
+                                      uint32_t** d_words, int64_t** d_tseg, int32_t** d_tanchor,
+                                      uint32_t** d_twords) {
+  if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
+  if (d_seg) *d_seg = A->pseg;
+  if (d_anchor) *d_anchor = A->panchor;
+  if (d_words) *d_words = A->pword;
+  if (d_tseg) *d_tseg = A->tseg;
+  if (d_tanchor) *d_tanchor = A->tanchor;
+  if (d_twords) *d_twords = A->tword;
+  return RAPTR_OK;
+}
+
 raptr_status raptr_matrix_drop_f32(raptr_matrix* A) {
   if (!A) return fail(RAPTR_ERR_INVALID, "matrix is null");
   if (!A->hval) return fail(RAPTR_ERR_INVALID, "the FP32 values are the only ones: call raptr_matrix_half first");
@@ -1446,6 +1583,7 @@ raptr_status raptr_matrix_bytes(const raptr_matrix* A, int64_t* bytes) {
   if (A->cnl) b += m * 4;
   if (A->rank) b += m * 8;
   if (A->hval) b += z * 4 + m * 8;
+  if (A->pword) b += (A->pwords + A->twords) * 4 + (m + 1) * 8 + m * 4 + (n + 1) * 8 + n * 4;
   *bytes = b;
   return RAPTR_OK;
 }

@@ -161,6 +161,25 @@ cudaError_t launch_sens_half(int64_t n, const int64_t* cp, const int32_t* trow, 
 cudaError_t launch_mlem_forward_half(int64_t m, const int64_t* rp, const int32_t* col, const uint16_t* hval,
                                      const float* rscale, const float* y, const float* x, const int32_t* rank,
                                      float* e, double* d_ll, cudaStream_t s, unsigned long long* next = nullptr);
+// Delta-coded FP16 runs (rows of the FP16 matrix or columns of its
+// transpose): word = (h << 16) | index step, runs starting on quads of four
+// words.  launch_pack_count writes the quads of each of the cnt runs of
+// (ptr, idx) into quads[0..cnt) (*bad |= 1 on a descending index);
+// launch_pack_fill writes the anchors and words of the runs, run r from
+// word 4*qoff[r] (qoff: the exclusive scan of the quads).
+cudaError_t launch_pack_count(int64_t cnt, const int64_t* ptr, const int32_t* idx, int64_t* quads, int32_t* bad,
+                              cudaStream_t s);
+cudaError_t launch_pack_fill(int64_t cnt, const int64_t* ptr, const int32_t* idx, const uint16_t* hv,
+                             const int64_t* qoff, int32_t* anchor, uint32_t* words, cudaStream_t s);
+// The FP16 passes over delta-coded runs (16-byte aligned words): as
+// launch_mlem_forward_half / launch_mlem_back_half, with `next` required
+// (an 8-byte counter, zero at launch).
+cudaError_t launch_mlem_forward_packed(int64_t m, const int64_t* seg, const int32_t* anchor, const uint32_t* words,
+                                       const float* rscale, const float* y, const float* x, const int32_t* rank,
+                                       float* e, double* d_ll, unsigned long long* next, cudaStream_t s);
+cudaError_t launch_mlem_back_packed(int64_t n, const int64_t* seg, const int32_t* anchor, const uint32_t* words,
+                                    const float* e, const float* x, const float* sens, float* out, double* d_acc,
+                                    bool update, unsigned long long* next, cudaStream_t s);
 // c_j = sum h_kj e_k, compensated; with update and `next` as launch_mlem_back.
 cudaError_t launch_mlem_back_half(int64_t n, const int64_t* cp, const int32_t* trow, const uint16_t* htval,
                                   const float* e, const float* x, const float* sens, float* out, double* d_acc,

@@ -375,6 +375,250 @@ __global__ void normalise_f64_kernel(int64_t n, double* __restrict__ x, const do
     x[i] = xx[i] * scale;
 }
 
+
+// ---- delta-coded FP16 form -------------------------------------------------
+//
+// Each row of the FP16 matrix (or column of its transpose) as a run of
+// 32-bit words, word = (h << 16) | d: h the entry's binary16 value, d the
+// step of its column (row position) from the previous word's index, the
+// first word's from the run's anchor, which is the first index (d = 0).  A
+// step above 65535 is split: words of step 65535 and value 0 come before
+// the entry's own word; words with value 0 (those, and the padding) make no
+// gather.  Runs start on 16-byte boundaries: offsets count
+// quads of four words, and the last quad is padded with words 0.  4 bytes
+// per entry instead of 6 (index 4 + value 2).
+//
+// A warp reads a run as quads, lane l taking quads l, l+32, ...: one
+// 16-byte load per four entries.  The indices follow from the steps by a
+// prefix sum: four steps within the lane, then across the lanes with a
+// warp scan of the lanes' sums, then across the warp's steps through the
+// carried last index.
+
+constexpr int kMaxStep = 65535;
+
+__device__ __forceinline__ int step_escapes(int d) { return d > kMaxStep ? (d - 1) / kMaxStep : 0; }
+
+// Words per run (entries plus escapes), as quads; *bad on a descending index.
+__global__ void __launch_bounds__(kThreads) pack_count_kernel(int64_t cnt, const int64_t* __restrict__ ptr,
+                                                             const int32_t* __restrict__ idx,
+                                                             int64_t* __restrict__ quads, int32_t* __restrict__ bad) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < cnt; r += nw) {
+    const int64_t b = ptr[r], e = ptr[r + 1];
+    int64_t words = 0;
+    for (int64_t k = b + lane; k < e; k += 32) {
+      const int d = k == b ? 0 : idx[k] - idx[k - 1];
+      if (d < 0) atomicOr(bad, 1);
+      words += 1 + step_escapes(d);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) words += __shfl_xor_sync(0xffffffffu, words, o);
+    if (lane == 0) quads[r] = (words + 3) >> 2;
+  }
+}
+
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+// The runs' anchors and words (run r from word 4*qoff[r]).
+__global__ void __launch_bounds__(kThreads) pack_fill_kernel(int64_t cnt, const int64_t* __restrict__ ptr,
+                                                            const int32_t* __restrict__ idx,
+                                                            const uint16_t* __restrict__ hv,
+                                                            const int64_t* __restrict__ qoff,
+                                                            int32_t* __restrict__ anchor,
+                                                            uint32_t* __restrict__ words) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < cnt; r += nw) {
+    const int64_t b = ptr[r], e = ptr[r + 1];
+    if (lane == 0) anchor[r] = e > b ? idx[b] : 0;
+    int64_t pos = qoff[r] * 4;
+    for (int64_t k0 = b; k0 < e; k0 += 32) {
+      const int64_t k = k0 + lane;
+      const int d = k < e ? (k == b ? 0 : idx[k] - idx[k - 1]) : 0;
+      const int esc = step_escapes(d);
+      const int c = k < e ? 1 + esc : 0;
+      const int incl = warp_incl_scan(c, lane);
+      int64_t w = pos + incl - c;
+      for (int j = 0; j < esc; j++) words[w++] = uint32_t(kMaxStep);
+      if (k < e) words[w] = (uint32_t(hv[k]) << 16) | uint32_t(d - esc * kMaxStep);
+      pos += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    for (int64_t w = pos + lane; w < qoff[r + 1] * 4; w += 32) words[w] = 0u;
+  }
+}
+
+__device__ __forceinline__ float word_h(uint32_t w) { return __half2float(__ushort_as_half(uint16_t(w >> 16))); }
+
+// v at the word's index, read only for a word with a value: the steps above
+// 65535 and the padding read nothing, so that a vector entry the run does
+// not hold (a ratio y/0 of a row without entries) cannot reach the sum.
+__device__ __forceinline__ float word_v(uint32_t w, const float* __restrict__ v, int i) {
+  return (w >> 16) ? __ldg(v + i) : 0.f;
+}
+
+// The indices of the QPL quads a[] the lanes hold (quad u of lane l is the
+// run's quad q + 32u + l), given the index before them (carry, updated to
+// the last index the warp's quads reach).  Steps of quads past the run's
+// end are 0.
+template <int QPL>
+__device__ __forceinline__ void quad_indices(const uint4 (&a)[QPL], int& carry, int lane, int (&i)[QPL][4]) {
+  int sum[QPL], incl[QPL];
+#pragma unroll
+  for (int u = 0; u < QPL; u++) {
+    sum[u] = int(a[u].x & 0xffffu) + int(a[u].y & 0xffffu) + int(a[u].z & 0xffffu) + int(a[u].w & 0xffffu);
+    incl[u] = sum[u];
+  }
+  // the QPL scans are independent; their latencies overlap
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+    for (int u = 0; u < QPL; u++) {
+      const int t = __shfl_up_sync(0xffffffffu, incl[u], o);
+      if (lane >= o) incl[u] += t;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < QPL; u++) {
+    const int b = carry + incl[u] - sum[u];
+    i[u][0] = b + int(a[u].x & 0xffffu);
+    i[u][1] = i[u][0] + int(a[u].y & 0xffffu);
+    i[u][2] = i[u][1] + int(a[u].z & 0xffffu);
+    i[u][3] = i[u][2] + int(a[u].w & 0xffffu);
+    carry += __shfl_sync(0xffffffffu, incl[u], 31);
+  }
+}
+
+constexpr int kPackedQuads = 4;  // quads per lane in flight (16 entries)
+
+// Loads the QPL quads of lane `lane` from quad q on (zeros past q1).
+template <int QPL>
+__device__ __forceinline__ void load_quads(const uint4* __restrict__ w, int64_t q, int64_t q1, int lane,
+                                           uint4 (&a)[QPL]) {
+#pragma unroll
+  for (int u = 0; u < QPL; u++) {
+    const int64_t k = q + 32 * u + lane;
+    a[u] = k < q1 ? __ldcs(w + k) : make_uint4(0u, 0u, 0u, 0u);
+  }
+}
+
+// Dot product of the run in quads [q0, q1) with v (FP32 accumulation).
+__device__ __forceinline__ float packed_row_dot(const uint4* __restrict__ w, int64_t q0, int64_t q1, int anchor,
+                                                const float* __restrict__ v, int lane) {
+  constexpr int Q = kPackedQuads;
+  float acc[Q];
+#pragma unroll
+  for (int u = 0; u < Q; u++) acc[u] = 0.f;
+  int carry = anchor;
+  for (int64_t q = q0; q < q1; q += 32 * Q) {
+    uint4 a[Q];
+    load_quads<Q>(w, q, q1, lane, a);
+    int i[Q][4];
+    quad_indices<Q>(a, carry, lane, i);
+#pragma unroll
+    for (int u = 0; u < Q; u++)
+      acc[u] += (word_h(a[u].x) * word_v(a[u].x, v, i[u][0]) + word_h(a[u].y) * word_v(a[u].y, v, i[u][1])) +
+                (word_h(a[u].z) * word_v(a[u].z, v, i[u][2]) + word_h(a[u].w) * word_v(a[u].w, v, i[u][3]));
+  }
+  float t = 0.f;
+#pragma unroll
+  for (int u = 0; u < Q; u++) t += acc[u];
+  return warp_sum_f(t);
+}
+
+// Column dot of a run with e, compensated as col_dot_half: each quad summed
+// in FP32 and added with a two-sum.
+__device__ __forceinline__ float packed_col_dot(const uint4* __restrict__ w, int64_t q0, int64_t q1, int anchor,
+                                                const float* __restrict__ ev, int lane) {
+  constexpr int Q = kPackedQuads;
+  float s = 0.f, c = 0.f;
+  int carry = anchor;
+  for (int64_t q = q0; q < q1; q += 32 * Q) {
+    uint4 a[Q];
+    load_quads<Q>(w, q, q1, lane, a);
+    int i[Q][4];
+    quad_indices<Q>(a, carry, lane, i);
+#pragma unroll
+    for (int u = 0; u < Q; u++)
+      two_sum_add(s, c, (word_h(a[u].x) * word_v(a[u].x, ev, i[u][0]) + word_h(a[u].y) * word_v(a[u].y, ev, i[u][1])) +
+                            (word_h(a[u].z) * word_v(a[u].z, ev, i[u][2]) + word_h(a[u].w) * word_v(a[u].w, ev, i[u][3])));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float so = __shfl_xor_sync(0xffffffffu, s, o);
+    const float co = __shfl_xor_sync(0xffffffffu, c, o);
+    two_sum_add(s, c, so);
+    c += co;
+  }
+  return s + c;
+}
+
+// The FP16 forward pass over delta-coded rows: e'[rank_i] = rscale_i * y_i /
+// (A x)_i, rows drawn kRowChunk at a time from `next` (zero at launch).
+__global__ void __launch_bounds__(kThreads) mlem_forward_packed_kernel(
+    int64_t m, const int64_t* __restrict__ seg, const int32_t* __restrict__ anchor, const uint4* __restrict__ words,
+    const float* __restrict__ rscale, const float* __restrict__ y, const float* __restrict__ x,
+    const int32_t* __restrict__ rank, float* __restrict__ e, double* __restrict__ ll, unsigned long long* next) {
+  const int lane = threadIdx.x & 31;
+  double ly = 0.0, lt = 0.0;
+  for (int64_t r0 = warp_next(next, lane) * kRowChunk; r0 < m; r0 = warp_next(next, lane) * kRowChunk)
+    for (int64_t r = r0, r1 = min(r0 + kRowChunk, m); r < r1; r++) {
+      const float yi = __ldg(y + r);
+      const int64_t dst = rank ? int64_t(__ldg(rank + r)) : r;
+      if (yi == 0.f) {
+        if (lane == 0) e[dst] = 0.f;
+        continue;
+      }
+      const float sc = __ldg(rscale + r);
+      const float yt = sc * packed_row_dot(words, seg[r], seg[r + 1], __ldg(anchor + r), x, lane);
+      if (lane == 0) {
+        e[dst] = sc * __fdiv_rn(yi, yt);
+        if (ll) {
+          ly += double(yi) * log(double(yt));
+          lt += double(yt);
+        }
+      }
+    }
+  if (ll) {
+    block_add_d(ly, ll);
+    __syncthreads();
+    block_add_d(lt, ll + 1);
+  }
+}
+
+// The FP16 back projection over delta-coded columns, columns drawn from
+// `next`; with UPDATE the MLEM update in the epilogue as mlem_back_half_kernel.
+template <bool UPDATE>
+__global__ void __launch_bounds__(kThreads) mlem_back_packed_kernel(
+    int64_t n, const int64_t* __restrict__ seg, const int32_t* __restrict__ anchor, const uint4* __restrict__ words,
+    const float* __restrict__ e, const float* __restrict__ x, const float* __restrict__ sens,
+    float* __restrict__ out, double* __restrict__ acc, unsigned long long* next) {
+  const int lane = threadIdx.x & 31;
+  double sum = 0.0;
+  for (int64_t j = warp_next(next, lane); j < n; j = warp_next(next, lane)) {
+    const float c = packed_col_dot(words, seg[j], seg[j + 1], __ldg(anchor + j), e, lane);
+    if (lane == 0) {
+      if (UPDATE) {
+        float dvs = sens[j];
+        dvs += float(dvs == 0.f);
+        const float xx = __fdiv_rn(__fmul_rn(x[j], c), dvs);
+        out[j] = xx;
+        sum += double(xx);
+      } else {
+        out[j] = c;
+      }
+    }
+  }
+  if (UPDATE) block_add_d(sum, acc);
+}
+
 }  // namespace
 
 cudaError_t launch_half_convert(int64_t m, int64_t nnz, const int64_t* rp, const float* val, const int32_t* trow,
@@ -431,6 +675,45 @@ cudaError_t launch_mlem_f64_iteration(int64_t m, int64_t n, const int64_t* rp, c
   mlem_back_f64_kernel<<<grid_rows(n), kThreads, 0, s>>>(n, cp, trow, tval, e, x, s64, xx, acc);
   normalise_f64_kernel<<<grid_elems(n), kThreads, 0, s>>>(n, x, xx, acc);
   note_launches(3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_count(int64_t cnt, const int64_t* ptr, const int32_t* idx, int64_t* quads, int32_t* bad,
+                              cudaStream_t s) {
+  if (cnt <= 0) return cudaSuccess;
+  pack_count_kernel<<<grid_rows(cnt), kThreads, 0, s>>>(cnt, ptr, idx, quads, bad);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_fill(int64_t cnt, const int64_t* ptr, const int32_t* idx, const uint16_t* hv,
+                             const int64_t* qoff, int32_t* anchor, uint32_t* words, cudaStream_t s) {
+  if (cnt <= 0) return cudaSuccess;
+  pack_fill_kernel<<<grid_rows(cnt), kThreads, 0, s>>>(cnt, ptr, idx, hv, qoff, anchor, words);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlem_forward_packed(int64_t m, const int64_t* seg, const int32_t* anchor, const uint32_t* words,
+                                       const float* rscale, const float* y, const float* x, const int32_t* rank,
+                                       float* e, double* d_ll, unsigned long long* next, cudaStream_t s) {
+  if (m <= 0) return cudaSuccess;
+  mlem_forward_packed_kernel<<<grid_rows(m), kThreads, 0, s>>>(
+      m, seg, anchor, reinterpret_cast<const uint4*>(words), rscale, y, x, rank, e, d_ll, next);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlem_back_packed(int64_t n, const int64_t* seg, const int32_t* anchor, const uint32_t* words,
+                                    const float* e, const float* x, const float* sens, float* out, double* d_acc,
+                                    bool update, unsigned long long* next, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const uint4* w = reinterpret_cast<const uint4*>(words);
+  if (update)
+    mlem_back_packed_kernel<true><<<grid_rows(n), kThreads, 0, s>>>(n, seg, anchor, w, e, x, sens, out, d_acc, next);
+  else
+    mlem_back_packed_kernel<false><<<grid_rows(n), kThreads, 0, s>>>(n, seg, anchor, w, e, x, sens, out, d_acc, next);
+  note_launches(1);
   return cudaGetLastError();
 }
 
