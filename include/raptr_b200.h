@@ -81,8 +81,8 @@ const char* raptr_last_error(void);
 int64_t raptr_kernel_launches(void);
 
 /* No counterpart in the reference (it frees its buffers with cudaFree).
- * Device blocks of 64 MB and more that the library frees (matrices, their
- * transposes, transpose staging, build scratch) are kept for reuse by its
+ * Device blocks that the library frees (matrices, their transposes,
+ * transpose staging, build scratch, counters) are kept for reuse by its
  * next allocations of a similar size, up to two thirds of each device's memory,
  * because freeing and reallocating tens of GB per reconstruction job costs
  * host time while the device idles.  Freeing still waits for the device's

@@ -2,12 +2,14 @@
 // transposes, transpose staging, build scratch), kept for reuse when freed.
 //
 // A reconstruction job allocates and frees tens of GB per build and
-// transpose; cudaFree of such blocks costs 30-600 ms of host time during
-// which the device idles, and a job that follows reallocates the same
-// sizes.  Blocks of at least kMinCached bytes are therefore not returned
-// to the driver when the library frees them but parked per device, and a
-// later request of a similar size (up to 25 % smaller) takes the smallest
-// fitting parked block.  Parked bytes per device are capped at two thirds
+// transpose, and a few dozen smaller blocks (row pointers, channel lists,
+// row orders, counters); cudaFree costs 30-600 ms of host time for the
+// large blocks and, at times, as much for a block of a few MB or bytes
+// (one transpose's release of its counters took 765 ms), during which the
+// device idles; a job that follows reallocates the same sizes.  Blocks are
+// therefore not returned to the driver when the library frees them but
+// parked per device, and a later request of a similar size (up to 25 %
+// smaller) takes the smallest fitting parked block.  Parked bytes per device are capped at two thirds
 // of the device's memory, which holds every block of a full reconstruction
 // job (matrix, transpose and the transpose's staging, ~107 GB at 70^3 x
 // 5.14M channels), so that the next job of the same size allocates nothing
@@ -37,16 +39,13 @@ namespace raptr {
 
 namespace {
 
-constexpr size_t kMinCached = size_t(64) << 20;
-
 struct Block {
   size_t bytes;
   int device;
 };
 
 std::mutex g_mu;
-std::unordered_map<void*, Block> g_live;                 // large blocks handed out
-std::unordered_map<void*, Block> g_small;                // smaller blocks handed out (counted only)
+std::unordered_map<void*, Block> g_live;                 // blocks handed out
 std::map<int, size_t> g_in_use;                          // device -> bytes handed out
 std::map<int, std::multimap<size_t, void*>> g_parked;    // device -> size -> block
 std::map<int, size_t> g_parked_bytes;
@@ -109,16 +108,6 @@ cudaError_t dev_alloc(void** p, size_t bytes) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (bytes < kMinCached) {
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!within_limit_locked(dev, bytes)) return cudaErrorMemoryAllocation;
-    e = cudaMalloc(p, bytes);
-    if (e == cudaSuccess) {
-      g_small[*p] = Block{bytes, dev};
-      g_in_use[dev] += bytes;
-    }
-    return e;
-  }
   std::lock_guard<std::mutex> lock(g_mu);
   auto& parked = g_parked[dev];
   auto it = parked.lower_bound(bytes);
@@ -131,12 +120,16 @@ cudaError_t dev_alloc(void** p, size_t bytes) {
     return cudaSuccess;
   }
   if (!within_limit_locked(dev, bytes)) return cudaErrorMemoryAllocation;
+  const double t0 = trace_on() ? trace_ms() : 0.0;
   e = cudaMalloc(p, bytes);
   if (e == cudaErrorMemoryAllocation && !parked.empty()) {
     (void)cudaGetLastError();
     release_locked(dev);
     e = cudaMalloc(p, bytes);
   }
+  if (trace_on())
+    trace("dev_alloc: %zu bytes from the driver in %.2f ms (%zu bytes parked on device %d)", bytes,
+          trace_ms() - t0, g_parked_bytes[dev], dev);
   if (e != cudaSuccess) {
     *p = nullptr;
     return e;
@@ -156,15 +149,10 @@ void dev_free(void* p) {
       b = it->second;
       g_live.erase(it);
       g_in_use[b.device] -= b.bytes;
-    } else {
-      auto si = g_small.find(p);
-      if (si != g_small.end()) {
-        g_in_use[si->second.device] -= si->second.bytes;
-        g_small.erase(si);
-      }
     }
   }
   if (b.bytes == 0) {
+    // not from dev_alloc
     cudaFree(p);
     return;
   }
@@ -174,7 +162,9 @@ void dev_free(void* p) {
   // Like cudaFree, wait for the device's work (which may still use the
   // block) before the block can be handed out again.  The wait runs without
   // the lock, so that other threads' allocations do not wait for it too.
+  const double t0 = trace_on() ? trace_ms() : 0.0;
   bool ok = cudaDeviceSynchronize() == cudaSuccess;
+  const double t1 = trace_on() ? trace_ms() : 0.0;
   size_t total = 0, freeb = 0;
   bool park = false;
   {
@@ -203,6 +193,9 @@ void dev_free(void* p) {
             cudaGetErrorString(e));
     }
   }
+  if (trace_on())
+    trace("dev_free: %zu bytes %s (device wait %.2f ms, then %.2f ms)", b.bytes,
+          park ? "parked" : "returned to the driver", t1 - t0, trace_ms() - t1);
   if (cur >= 0 && cur != b.device) cudaSetDevice(cur);
 }
 

@@ -17,8 +17,8 @@ raptr_status set_error(raptr_status st, const std::string& msg);
 void note_launches(long long k);
 long long launches_so_far();
 
-// Device allocations of the library (devmem.cpp): blocks of 64 MB and more
-// are parked for reuse when freed instead of going back to the driver;
+// Device allocations of the library (devmem.cu): blocks are parked for
+// reuse when freed instead of going back to the driver;
 // dev_free waits for the device like cudaFree.  dev_release returns the
 // parked blocks of a device (-1: all) to the driver.
 cudaError_t dev_alloc(void** p, size_t bytes);
