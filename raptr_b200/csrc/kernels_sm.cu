@@ -166,8 +166,9 @@ struct DenseIndex {
 // general loop, which adds through emit(ix, iy, iz, L): a ray parallel to
 // the planes of some axis (start and end coordinate equal) leaves that axis
 // unconstrained, as the reference's masked min/max does, and every
-// candidate voxel along it gets the length.
-template <bool OISO, class Emit, class Index>
+// candidate voxel along it gets the length.  UNROLL is the step loop's
+// unroll factor (the arithmetic of each step is the same for any).
+template <bool OISO, int UNROLL, class Emit, class Index>
 __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, const float r[6], int part, Emit& emit,
                                          Index& ix, int* bad_walk) {
   float dir[3];
@@ -352,7 +353,7 @@ __device__ __forceinline__ void walk_ray(const DGeom& g, const Channel& ch, cons
     const float sq1 = float(step[1] > 0 ? s1 + 2 : 1 - s1);
     const float sq2 = float(step[2] > 0 ? s2 + 2 : 1 - s2);
     const float sprev = fmaxf(sl0, fmaxf(sl1, sl2));
-#pragma unroll 1
+#pragma unroll UNROLL
     for (int it = 0; it < guard_max; it++) {
       const float a_hi = fminf(hi0, fminf(hi1, hi2));
       // A voxel between two planes at the same parameter gets length 0; it
@@ -528,6 +529,14 @@ __device__ inline void slab_window(const DGeom& g, int a, const float plo[3], co
   *ihi = max(lo, hi);
 }
 
+// The dense kernel's step-loop unroll factor by row capacity, measured on
+// full builds: 6 at H = 4096 (70^3 x 5.14M channels: 2.04 s unrolled 1,
+// 2.00 s by 2, 1.86 s by 4, 1.81 s by 6 and by 8; 8 spills), none at
+// H = 8192 (100^3 x 1.71M channels: 1.23 s unrolled 1, 1.25 s by 4, 1.32 s
+// by 6, 1.37 s by 8) nor at H = 2048 (40^3 x 143K channels: 8-9 ms either
+// way, and unrolled it spills).
+constexpr int dense_walk_unroll(int H) { return H == 4096 ? 6 : 1; }
+
 // Row status the dense kernel leaves for the table kernel: the row is to be
 // built with the hash table (it does not qualify for dense windows, or a
 // ray left its windows).
@@ -699,7 +708,7 @@ __global__ void __launch_bounds__(T) sm_dense_kernel(DGeom g, const float2* __re
         float r[6];
         make_ray(ch, seed, cnl, ray, r);
         if (sdir > 0 ? !(RFSUB(r[3], r[0]) > 0.f) : !(RFSUB(r[3], r[0]) < 0.f)) dense_fail = 1;
-        walk_ray<OISO>(g, ch, r, part, emit, dix, &bad_walk);
+        walk_ray<OISO, dense_walk_unroll(H)>(g, ch, r, part, emit, dix, &bad_walk);
       }
     } else {
       DenseIndex<2> dix{acc, sbase, sdk, wv, nslots};
@@ -707,7 +716,7 @@ __global__ void __launch_bounds__(T) sm_dense_kernel(DGeom g, const float2* __re
         float r[6];
         make_ray(ch, seed, cnl, ray, r);
         if (sdir > 0 ? !(RFSUB(r[5], r[2]) > 0.f) : !(RFSUB(r[5], r[2]) < 0.f)) dense_fail = 1;
-        walk_ray<OISO>(g, ch, r, part, emit, dix, &bad_walk);
+        walk_ray<OISO, dense_walk_unroll(H)>(g, ch, r, part, emit, dix, &bad_walk);
       }
     }
   }
@@ -881,7 +890,7 @@ __global__ void __launch_bounds__(T) sm_table_kernel(DGeom g, const float2* __re
         } else {
           make_ray(ch, seed, cnl, ray, r);
         }
-        walk_ray<OISO>(g, ch, r, part, emit, kix, &bad_walk);
+        walk_ray<OISO, 1>(g, ch, r, part, emit, kix, &bad_walk);
       }
     }
     __syncthreads();
