@@ -64,7 +64,7 @@ TRAFFIC_BYTES_PER_ENTRY = {
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["raptr", "reference"], default="raptr")
     p.add_argument("--workload", choices=list(cfg.WORKLOADS), default="full")

@@ -1143,14 +1143,9 @@ raptr_status raptr_sensitivity(int64_t m, int64_t n, const int64_t* d_row_ptr, c
   cudaStream_t s = as_stream(stream);
   RCU(cudaMemsetAsync(d_s64, 0, size_t(n) * sizeof(double), s));
   RCU(launch_column_sums(m, d_row_ptr, d_col, d_val, d_s64, s));
-  if (d_s32) {
-    double* acc = nullptr;
-    RCU(cudaMallocAsync(&acc, sizeof(double), s));
-    cudaError_t e = launch_sum_f64(d_s64, n, acc, s);
-    if (e == cudaSuccess) e = launch_sens_normalise(n, d_s64, acc, d_s32, s);
-    cudaFreeAsync(acc, s);
-    if (e != cudaSuccess) return cuda_fail(e, "sensitivity normalisation");
-  }
+  // no device scratch for the sum: a stream-ordered allocation here took
+  // from microseconds to hundreds of milliseconds of host time
+  if (d_s32) RCU(launch_sens_normalise_self(n, d_s64, d_s32, s));
   return RAPTR_OK;
 }
 
@@ -1290,6 +1285,7 @@ raptr_status mlem_impl(raptr_ctx* ctx, int64_t m, int64_t n, const MlemArrays& A
   if (!use_graph) {
     RCU(enqueue(s));
   } else {
+    const double tg0 = trace_on() ? trace_ms() : 0.0;
     cudaStream_t cap;
     RCU(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaEvent_t ev;
@@ -1305,17 +1301,20 @@ raptr_status mlem_impl(raptr_ctx* ctx, int64_t m, int64_t n, const MlemArrays& A
       e = (e1 != cudaSuccess) ? e1 : e2;
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-    if (trace_on()) trace("mlem: %d iterations captured and instantiated", int(n_iter));
+    const double tg1 = trace_on() ? trace_ms() : 0.0;
+    if (trace_on()) trace("mlem: %d iterations captured and instantiated in %.2f ms", int(n_iter), tg1 - tg0);
     if (e == cudaSuccess) e = cudaGraphLaunch(exec, cap);
     // the launches were counted when they were captured; the graph runs
     // each of them once
     if (e == cudaSuccess) e = cudaEventRecord(ev, cap);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cap);
+    const double tg2 = trace_on() ? trace_ms() : 0.0;
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     cudaEventDestroy(ev);
     cudaStreamDestroy(cap);
+    if (trace_on()) trace("mlem: graph ran in %.2f ms, released in %.2f ms", tg2 - tg1, trace_ms() - tg2);
     if (e != cudaSuccess) return cuda_fail(e, "MLEM graph");
   }
   if (want_times) {
@@ -1594,14 +1593,7 @@ raptr_status raptr_sensitivity_half(int64_t n, const int64_t* d_col_ptr, const i
   if (n <= 0 || !d_col_ptr || !d_s64) return fail(RAPTR_ERR_INVALID, "bad argument");
   cudaStream_t s = as_stream(stream);
   RCU(launch_sens_half(n, d_col_ptr, d_row_idx, d_htval, d_pscale, d_s64, s));
-  if (d_s32) {
-    double* acc = nullptr;
-    RCU(cudaMallocAsync(&acc, sizeof(double), s));
-    cudaError_t e = launch_sum_f64(d_s64, n, acc, s);
-    if (e == cudaSuccess) e = launch_sens_normalise(n, d_s64, acc, d_s32, s);
-    cudaFreeAsync(acc, s);
-    if (e != cudaSuccess) return cuda_fail(e, "sensitivity normalisation");
-  }
+  if (d_s32) RCU(launch_sens_normalise_self(n, d_s64, d_s32, s));
   return RAPTR_OK;
 }
 
@@ -1916,11 +1908,7 @@ raptr_status raptr_mlem_stream(raptr_ctx* ctx, const int32_t* d_cnl, int64_t n_l
       it = -1;
       continue;
     }
-    if (first && s64) {
-      RCU(cudaMemsetAsync(acc + 1, 0, sizeof(double), s));
-      RCU(launch_sum_f64(s64, N, acc + 1, s));
-      RCU(launch_sens_normalise(N, s64, acc + 1, s32, s));
-    }
+    if (first && s64) RCU(launch_sens_normalise_self(N, s64, s32, s));
     if (first && d_s_out) RCU(cudaMemcpyAsync(d_s_out, s_use, size_t(N) * sizeof(float), cudaMemcpyDeviceToDevice, s));
     RCU(cudaMemsetAsync(acc, 0, sizeof(double), s));
     RCU(launch_mlem_update(N, d_x, c, s_use, acc, s));
@@ -2052,11 +2040,9 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
     RSTEP(cudaMemcpyAsync(d_x, h_x0, size_t(N) * sizeof(float), cudaMemcpyHostToDevice, s));
     h2d += N * int64_t(sizeof(float));
   } else {
-    // Uniform image normalised to sum 1 (src/tests/reco.cu:145-158).
-    std::vector<float> ones(size_t(N), float(1. / float(N)));
-    RSTEP(cudaMemcpyAsync(d_x, ones.data(), size_t(N) * sizeof(float), cudaMemcpyHostToDevice, s));
-    RSTEP(cudaStreamSynchronize(s));
-    h2d += N * int64_t(sizeof(float));
+    // Uniform image normalised to sum 1 (src/tests/reco.cu:145-158),
+    // filled on the device
+    RSTEP(launch_fill(d_x, float(1. / float(N)), N, s));
   }
   RSTEP(cudaEventRecord(ev[4], s));
   trace("reco_host: sensitivity");

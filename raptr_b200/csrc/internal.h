@@ -123,7 +123,8 @@ cudaError_t launch_scales(float* x, float alpha, int64_t n, cudaStream_t s);
 cudaError_t launch_sum(const float* x, int64_t n, double* d_acc, cudaStream_t s);
 cudaError_t launch_column_sums(int64_t m, const int64_t* rp, const int32_t* col, const float* val, double* s64,
                                cudaStream_t s);
-cudaError_t launch_sens_normalise(int64_t n, const double* s64, const double* d_total, float* s32, cudaStream_t s);
+// s32 = s64 / sum(s64) with the sum taken inside (one CTA, fixed order).
+cudaError_t launch_sens_normalise_self(int64_t n, const double* s64, float* s32, cudaStream_t s);
 cudaError_t launch_sum_f64(const double* x, int64_t n, double* d_acc, cudaStream_t s);
 
 // c += A^T (y / (A x)); when d_ll is non-null, d_ll[0] += sum y*log(Ax),
@@ -287,6 +288,7 @@ cudaError_t launch_mlem_back(int64_t n, const int64_t* cp, const int32_t* trow, 
                              const float* x, const float* sens, float* out, double* d_acc, bool update,
                              cudaStream_t s, unsigned long long* next = nullptr);
 cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s);
+cudaError_t launch_fill(float* p, float v, int64_t n, cudaStream_t s);
 cudaError_t launch_narrow_i64(const int64_t* in, int64_t n, int32_t* out, cudaStream_t s);
 cudaError_t launch_widen_i32(const int32_t* in, int64_t n, int64_t* out, cudaStream_t s);
 

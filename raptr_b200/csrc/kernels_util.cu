@@ -123,6 +123,11 @@ __global__ void iota_kernel(int32_t* __restrict__ p, int64_t n) {
     p[i] = int32_t(i);
 }
 
+__global__ void fill_kernel(float* __restrict__ p, float v, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    p[i] = v;
+}
+
 __global__ void narrow_kernel(const int64_t* __restrict__ in, int64_t n, int32_t* __restrict__ out) {
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
     out[i] = int32_t(in[i]);
@@ -145,6 +150,14 @@ unsigned grid_for(int64_t n, int threads) {
 cudaError_t launch_iota(int32_t* p, int64_t n, cudaStream_t s) {
   if (n > 0) {
     iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, n);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill(float* p, float v, int64_t n, cudaStream_t s) {
+  if (n > 0) {
+    fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, v, n);
     note_launches(1);
   }
   return cudaGetLastError();

@@ -180,6 +180,12 @@ struct raptr_server {
   std::map<std::string, std::unique_ptr<raptr::Entry>> entries;
   raptr::LruBudget<std::string> cache{0};
   int64_t state_bytes = 0;  // measurement vectors of running requests
+  // the requests' measurement vectors come from this pool, which keeps
+  // freed memory for the next request (the default pool hands it back to
+  // the driver at each synchronisation, and mapping it again cost up to
+  // hundreds of milliseconds of the scheduler's time); trimmed when a
+  // matrix is dropped
+  cudaMemPool_t pool = nullptr;
   raptr_server_stats st{};
 
   void loop();
@@ -273,6 +279,7 @@ raptr_status raptr_server::build(Entry* e, std::string* err) {
 void raptr_server::drop(Entry* e) {
   DeviceScope ds(device);
   if (e->stream) cudaStreamSynchronize(e->stream);
+  if (pool) cudaMemPoolTrimTo(pool, 0);
   cudaFree(e->Xbuf[0]);
   cudaFree(e->Xbuf[1]);
   cudaFree(e->Y);
@@ -443,7 +450,8 @@ bool raptr_server::admit(std::unique_lock<std::mutex>& lk) {
     // measurement on the device (stream-ordered allocation: no device-wide
     // synchronisation while other batches run)
     DeviceScope ds(device);
-    cudaError_t ce = cudaMallocAsync(&r->y_dev, size_t(e->m) * sizeof(float), e->stream);
+    cudaError_t ce = pool ? cudaMallocFromPoolAsync(&r->y_dev, size_t(e->m) * sizeof(float), pool, e->stream)
+                          : cudaMallocAsync(&r->y_dev, size_t(e->m) * sizeof(float), e->stream);
     if (ce == cudaSuccess)
       ce = cudaMemcpyAsync(r->y_dev, r->y_host.data(), size_t(e->m) * sizeof(float), cudaMemcpyHostToDevice,
                            e->stream);
@@ -588,6 +596,20 @@ raptr_status raptr_server_create(int32_t device, const raptr_server_opts* opts, 
   s->device = device;
   s->opts = *opts;
   s->cache = LruBudget<std::string>(opts->hbm_budget_bytes);
+  {
+    DeviceScope ds(device);
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&s->pool, &props) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+      (void)cudaGetLastError();
+      s->pool = nullptr;  // the default pool then
+    }
+  }
   s->worker = std::thread([s] { s->loop(); });
   *out = s;
   return RAPTR_OK;
@@ -608,6 +630,11 @@ raptr_status raptr_server_destroy(raptr_server* s) {
     cudaFree(r->y_dev);
   }
   for (auto& kv : s->entries) s->drop(kv.second.get());
+  if (s->pool) {
+    DeviceScope ds(s->device);
+    cudaDeviceSynchronize();
+    cudaMemPoolDestroy(s->pool);
+  }
   s->cv_done.notify_all();
   delete s;
   return RAPTR_OK;
