@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define RAPTR_ABI_VERSION 5
+#define RAPTR_ABI_VERSION 6
 
 typedef enum raptr_status {
   RAPTR_OK = 0,
@@ -234,6 +234,11 @@ raptr_status raptr_sum(const float* d_x, int64_t n, double* sum_out, void* strea
  * d_s32 is non-null, the same image normalised to sum 1 in float. */
 raptr_status raptr_sensitivity(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
                                const float* d_val, double* d_s64, float* d_s32, void* stream);
+/* The same through the transpose (its column pointers and values): no
+ * atomics, so the sums come out the same on every run; about six times
+ * faster than the CSR form at 70^3 x 5.14M channels. */
+raptr_status raptr_sensitivity_csc(int64_t n, const int64_t* d_col_ptr, const float* d_tval, double* d_s64,
+                                   float* d_s32, void* stream);
 
 typedef struct raptr_mlem_opts {
   int32_t use_graph;   /* capture the iteration loop in a CUDA graph            */

@@ -151,6 +151,7 @@ _SIGNATURES = {
     "raptr_matrix_half": (C.c_int, [VP, VP]),
     "raptr_matrix_half_info": (C.c_int, [VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), C.POINTER(VP)]),
     "raptr_sensitivity_half": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, VP]),
+    "raptr_sensitivity_csc": (C.c_int, [I64, VP, VP, VP, VP, VP]),
     "raptr_mlem_half": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, I32,
                                   C.POINTER(raptr_mlem_opts), VP]),
     "raptr_pack_half": (C.c_int, [I64, VP, VP, VP, VP, VP, VP, I64, C.POINTER(I64), VP]),
@@ -656,13 +657,19 @@ def spmv(op: int, m: int, n: int, row_ptr, col, val, x, alpha=1.0, beta=0.0, y=N
     return y
 
 
-def sensitivity(A: Matrix, stream=None):
-    """(FP64 column sums, FP32 image normalised to sum 1)."""
+def sensitivity(A: Matrix, stream=None, use_transpose: bool = True):
+    """(FP64 column sums, FP32 image normalised to sum 1), through A's
+    transpose when it has one (raptr_sensitivity_csc) unless use_transpose
+    is False."""
     torch = _torch()
     s64 = torch.empty(A.n, dtype=torch.float64, device=A.row_ptr.device)
     s32 = torch.empty(A.n, dtype=torch.float32, device=A.row_ptr.device)
-    _check(lib().raptr_sensitivity(A.m, A.n, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(s64), _ptr(s32),
-                                   _stream(stream)))
+    if use_transpose and A.has_transpose and A.tval is not None:
+        _check(lib().raptr_sensitivity_csc(A.n, _ptr(A.col_ptr), _ptr(A.tval), _ptr(s64), _ptr(s32),
+                                           _stream(stream)))
+    else:
+        _check(lib().raptr_sensitivity(A.m, A.n, _ptr(A.row_ptr), _ptr(A.col), _ptr(A.val), _ptr(s64), _ptr(s32),
+                                       _stream(stream)))
     return s64, s32
 
 

@@ -1137,6 +1137,15 @@ raptr_status raptr_sum(const float* d_x, int64_t n, double* sum_out, void* strea
 
 // ---- sensitivity and MLEM -------------------------------------------------------------
 
+raptr_status raptr_sensitivity_csc(int64_t n, const int64_t* d_col_ptr, const float* d_tval, double* d_s64,
+                                   float* d_s32, void* stream) {
+  if (n <= 0 || !d_col_ptr || !d_s64) return fail(RAPTR_ERR_INVALID, "bad argument");
+  cudaStream_t s = as_stream(stream);
+  RCU(launch_column_sums_csc(n, d_col_ptr, d_tval, d_s64, s));
+  if (d_s32) RCU(launch_sens_normalise_self(n, d_s64, d_s32, s));
+  return RAPTR_OK;
+}
+
 raptr_status raptr_sensitivity(int64_t m, int64_t n, const int64_t* d_row_ptr, const int32_t* d_col,
                                const float* d_val, double* d_s64, float* d_s32, void* stream) {
   if (m < 0 || n <= 0 || !d_row_ptr || !d_s64) return fail(RAPTR_ERR_INVALID, "bad argument");
@@ -2023,7 +2032,7 @@ raptr_status raptr_reco_host(const raptr_geom* geom, int device, const float* h_
   if (!h_sens) {
     if (!streamed) {
       RSTEP(dev_malloc(&d_s64, size_t(N) * sizeof(double)));
-      st = raptr_sensitivity(A->m, N, A->rp, A->col, A->val, d_s64, d_s, s);
+      st = raptr_sensitivity_csc(N, A->cp, A->tval, d_s64, d_s, s);
       RSTATUS();
     }
   } else {

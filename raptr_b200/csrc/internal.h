@@ -123,6 +123,8 @@ cudaError_t launch_scales(float* x, float alpha, int64_t n, cudaStream_t s);
 cudaError_t launch_sum(const float* x, int64_t n, double* d_acc, cudaStream_t s);
 cudaError_t launch_column_sums(int64_t m, const int64_t* rp, const int32_t* col, const float* val, double* s64,
                                cudaStream_t s);
+// s64[j] = sum of column j through the transpose (warp per column, no atomics).
+cudaError_t launch_column_sums_csc(int64_t n, const int64_t* cp, const float* tval, double* s64, cudaStream_t s);
 // s32 = s64 / sum(s64) with the sum taken inside (one CTA, fixed order).
 cudaError_t launch_sens_normalise_self(int64_t n, const double* s64, float* s32, cudaStream_t s);
 cudaError_t launch_sum_f64(const double* x, int64_t n, double* d_acc, cudaStream_t s);

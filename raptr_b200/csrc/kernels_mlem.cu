@@ -244,6 +244,22 @@ __global__ void __launch_bounds__(kThreads) colsum_kernel(int64_t m, const int64
   }
 }
 
+// The same column sums through the transpose: a warp per column, lanes on
+// strided entries summed in FP64 and combined in a fixed order (no atomics,
+// the same result on every run); the values stream once (4 bytes per entry).
+__global__ void __launch_bounds__(kThreads) colsum_csc_kernel(int64_t n, const int64_t* __restrict__ cp,
+                                                              const float* __restrict__ tval,
+                                                              double* __restrict__ s) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t j = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; j < n; j += nw) {
+    double a = 0.0;
+    for (int64_t k = cp[j] + lane; k < cp[j + 1]; k += 32) a += double(__ldcs(tval + k));
+    a = warp_sum_d(a);
+    if (lane == 0) s[j] = a;
+  }
+}
+
 // s32 = s64 / sum(s64) in one CTA of kNormThreads: the FP64 sum in a fixed
 // order (each thread's stride, then a tree over the threads), so the result
 // does not depend on scheduling, and no device scratch is needed.  Reads
@@ -645,6 +661,14 @@ cudaError_t launch_column_sums(int64_t m, const int64_t* rp, const int32_t* col,
                                cudaStream_t s) {
   if (m > 0) {
     colsum_kernel<<<row_grid(m), kThreads, 0, s>>>(m, rp, col, val, s64);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_column_sums_csc(int64_t n, const int64_t* cp, const float* tval, double* s64, cudaStream_t s) {
+  if (n > 0) {
+    colsum_csc_kernel<<<row_grid(n), kThreads, 0, s>>>(n, cp, tval, s64);
     note_launches(1);
   }
   return cudaGetLastError();

@@ -30,7 +30,7 @@ def test_python_layer_binds_every_declared_symbol(rlib):
 
 def test_abi_version_and_error_string(rlib):
     L = rlib.lib()
-    assert L.raptr_abi_version() == 5
+    assert L.raptr_abi_version() == 6
     assert isinstance(L.raptr_last_error(), bytes)
 
 

@@ -278,9 +278,25 @@ def test_coo2csr_and_ecsr_known_answers(rlib, torch):
     assert e.cpu().tolist() == [0, 3, 3, 5]
 
 
-def test_sensitivity_fp64(rlib, oracle, small_full_matrix):
+def sensitivity_csc(rlib, torch, A):
+    """raptr_sensitivity_csc over a transpose of A's arrays (caller buffers,
+    so that the shared matrix keeps no transpose)."""
+    cp, _, tv = rlib.csr_transpose(A.m, A.n, A.row_ptr, A.col, A.val)
+    s64 = torch.empty(A.n, dtype=torch.float64, device="cuda")
+    s32 = torch.empty(A.n, dtype=torch.float32, device="cuda")
+    rlib._check(rlib.lib().raptr_sensitivity_csc(A.n, cp.data_ptr(), tv.data_ptr(), s64.data_ptr(), s32.data_ptr(),
+                                                 None))
+    return s64, s32
+
+
+@pytest.mark.parametrize("through", ["rows", "transpose"])
+def test_sensitivity_fp64(rlib, oracle, torch, small_full_matrix, through):
     A, (rp, col, val), lst = small_full_matrix
-    s64, s32 = rlib.sensitivity(A)
+    assert not A.has_transpose
+    if through == "transpose":
+        s64, s32 = sensitivity_csc(rlib, torch, A)
+    else:
+        s64, s32 = rlib.sensitivity(A)
     s64 = s64.cpu().numpy()
     # against the column sums of the same (GPU) values: FP64 sums in another order
     rp_g, col_g, val_g = A.to_numpy()
@@ -290,6 +306,10 @@ def test_sensitivity_fp64(rlib, oracle, small_full_matrix):
     # against the oracle's matrix: values agree to 1e-5, so do the sums
     want_o = oracle.column_sums_f64(A.m, A.n, rp, col, val)
     assert np.max(np.abs(s64 - want_o)) <= 1e-5 * want_o.max()
+    if through == "transpose":
+        # no atomics: the same bits on every run
+        again, _ = sensitivity_csc(rlib, torch, A)
+        assert np.array_equal(again.cpu().numpy(), s64)
 
 
 # ---------------------------------------------------------------- MLEM
