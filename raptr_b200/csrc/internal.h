@@ -222,6 +222,9 @@ struct BatchArgs {
   const int32_t* seg = nullptr;
   int seg_blocks = 0;
   float* P = nullptr;
+  // n x the largest tile floats (may be null): a tile narrower than the
+  // batch gathers its images from a compact copy here
+  float* Xt = nullptr;
 };
 // The row-block offsets of every column of a transpose (see BatchArgs.seg):
 // seg[j*(B+1) + b] = offset in column j of its first entry with row >= b*m/B.

@@ -3,9 +3,14 @@
 // entry is read once per frame tile instead of once per frame.
 //
 // Layout: images X (n x K) and measurements Y (m x K) are frame-minor
-// (X[j*K + f]); the ratios E (m x K) sit at the rows' positions in the
-// transpose's order, like the single-frame e.  A pass handles a tile of KT
-// consecutive frames.  Within a warp, lanes split into EPW entry slots of
+// (X[j*K + f]); the ratios E sit at the rows' positions in the transpose's
+// order, like the single-frame e, in one block per tile: the tile of KT
+// frames from f0 holds E[f0*m + k*KT + (f - f0)], so that the back pass
+// over a tile gathers from m*KT floats (82 MB for 4 frames at 5.14M rows,
+// inside L2) instead of 16 bytes out of each row of an m x K array, whose
+// sectors for a 4-frame tile spread over 164 MB and missed L2 (33 ms per
+// 4-frame back pass, against 3.9 ms for one frame).  A pass handles a tile
+// of KT consecutive frames.  Within a warp, lanes split into EPW entry slots of
 // LPE lanes, each lane owning VEC frames (LPE*VEC = KT, EPW*LPE = 32): per
 // step a warp reads EPW matrix entries and gathers EPW rows of KT frames,
 // coalesced.  The value type is binary16 (with the per-row scale folded
@@ -39,6 +44,10 @@ unsigned grid_warps(int64_t items) {
 }
 
 constexpr int kColsPerWarp = 48;  // back pass: columns a warp takes before its block ends
+// CTAs per SM both passes are compiled for: with 5 (48 registers) the back
+// pass runs 10-35 % faster for every frame tile than compiled without a
+// bound (40 registers, 6 CTAs per SM), the forward pass 1-6 % (8: slower)
+constexpr int kBatchBlocks = 5;
 constexpr double kBackGroupBytes = 48.0 * (1 << 20);  // ratios of a back-pass row-block group
 
 __device__ __forceinline__ float to_f(float v) { return v; }
@@ -61,22 +70,27 @@ __device__ __forceinline__ void fma4(float (&a)[4], float w, float4 x) {
   a[3] += w * x.w;
 }
 
-// Forward: E[rank_i*K + f] = sc_i * Y[i*K + f] / (sc_i * sum_j v_ij X[j*K + f])
-// for the frames f of the tile (0 where Y == 0); sc = rscale (FP16) or 1.
+// Forward: Et[rank_i*KT + f - f0] = sc_i * Y[i*K + f] / (sc_i * sum_j v_ij
+// X[j*K + f]) for the frames f of the tile (0 where Y == 0), Et = E + f0*m
+// the tile's block of ratios; sc = rscale (FP16) or 1.  The images are gathered from Xg with row stride xs:
+// X + f0 and K, or a compact copy of the tile's frames and KT (a 4-frame
+// tile then gathers from n*16 bytes instead of 16 bytes of each 256-byte
+// row of a 64-frame X).
 template <int KT, typename VT>
-__global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int K, int f0,
+__global__ void __launch_bounds__(kThreads, kBatchBlocks) batch_forward_kernel(int64_t m, int K, int f0,
                                                                  const int64_t* __restrict__ rp,
                                                                  const int32_t* __restrict__ col,
                                                                  const VT* __restrict__ val,
                                                                  const float* __restrict__ rscale,
                                                                  const float* __restrict__ Y,
-                                                                 const float* __restrict__ X,
+                                                                 const float* __restrict__ Xg, int xs,
                                                                  const int32_t* __restrict__ rank,
-                                                                 float* __restrict__ E) {
+                                                                 float* __restrict__ Et) {
   using S = Split<KT>;
   const int lane = threadIdx.x & 31;
   const int es = lane / S::LPE, fg = lane % S::LPE;
   const int fbase = f0 + fg * S::VEC;
+  const float* __restrict__ X = Xg + fg * S::VEC;  // the lane's four frames
   const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
   for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
     float acc[S::VEC];
@@ -88,12 +102,12 @@ __global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int 
     for (; k + S::EPW < e; k += 2 * S::EPW) {
       const int c0 = __ldg(col + k), c1 = __ldg(col + k + S::EPW);
       const float w0 = to_f(val[k]), w1 = to_f(val[k + S::EPW]);
-      const float4 x0 = ld4(X + int64_t(c0) * K + fbase);
-      const float4 x1 = ld4(X + int64_t(c1) * K + fbase);
+      const float4 x0 = ld4(X + int64_t(c0) * xs);
+      const float4 x1 = ld4(X + int64_t(c1) * xs);
       fma4(acc, w0, x0);
       fma4(acc, w1, x1);
     }
-    if (k < e) fma4(acc, to_f(val[k]), ld4(X + int64_t(__ldg(col + k)) * K + fbase));
+    if (k < e) fma4(acc, to_f(val[k]), ld4(X + int64_t(__ldg(col + k)) * xs));
 #pragma unroll
     for (int o = S::LPE; o < 32; o <<= 1)
 #pragma unroll
@@ -104,14 +118,15 @@ __global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int 
 #pragma unroll
       for (int v = 0; v < S::VEC; v++) {
         const float yi = __ldg(Y + r * K + fbase + v);
-        E[dst * K + fbase + v] = yi == 0.f ? 0.f : sc * __fdiv_rn(yi, sc * acc[v]);
+        Et[dst * KT + fg * S::VEC + v] = yi == 0.f ? 0.f : sc * __fdiv_rn(yi, sc * acc[v]);
       }
     }
   }
 }
 
 // Back projection and update for the frames of the tile:
-// c = sum_k v_kj E[k*K + f] (FP32; the FP16 values dominate its error),
+// c = sum_k v_kj Eb[k*KT + f - f0] (Eb = E + f0*m, the tile's block of
+// ratios; FP32, the FP16 values dominate its error),
 // XX = X*c/(S+(S==0)), acc[f] += sum_j XX (FP64).  Warps take columns from
 // the counter *next (zero at launch).
 //
@@ -123,11 +138,11 @@ __global__ void __launch_bounds__(kThreads) batch_forward_kernel(int64_t m, int 
 // last group adds them and finishes as above.  mode: 0 = the whole column
 // at once, 1 = first group, 2 = a middle group, 3 = the last group.
 template <int KT, typename VT>
-__global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, int f0, unsigned long long* next,
+__global__ void __launch_bounds__(kThreads, kBatchBlocks) batch_back_kernel(int64_t n, int K, int f0, unsigned long long* next,
                                                               const int64_t* __restrict__ cp,
                                                               const int32_t* __restrict__ trow,
                                                               const VT* __restrict__ tval,
-                                                              const float* __restrict__ E,
+                                                              const float* __restrict__ Eb,
                                                               const float* __restrict__ X,
                                                               const float* __restrict__ sens,
                                                               const int32_t* __restrict__ col_order,
@@ -139,6 +154,8 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
   const int es = lane / S::LPE, fg = lane % S::LPE;
   const int fbase = f0 + fg * S::VEC;
   const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  // the lane's four frames of this tile's block of ratios
+  const float* __restrict__ Et = Eb + fg * S::VEC;
   double fsum[S::VEC];
 #pragma unroll
   for (int v = 0; v < S::VEC; v++) fsum[v] = 0.0;
@@ -166,12 +183,12 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
     for (; p + S::EPW < e; p += 2 * S::EPW) {
       const int k0 = __ldg(trow + p), k1 = __ldg(trow + p + S::EPW);
       const float w0 = to_f(tval[p]), w1 = to_f(tval[p + S::EPW]);
-      const float4 e0 = ld4(E + int64_t(k0) * K + fbase);
-      const float4 e1 = ld4(E + int64_t(k1) * K + fbase);
+      const float4 e0 = ld4(Et + int64_t(k0) * KT);
+      const float4 e1 = ld4(Et + int64_t(k1) * KT);
       fma4(s, w0, e0);
       fma4(s, w1, e1);
     }
-    if (p < e) fma4(s, to_f(tval[p]), ld4(E + int64_t(__ldg(trow + p)) * K + fbase));
+    if (p < e) fma4(s, to_f(tval[p]), ld4(Et + int64_t(__ldg(trow + p)) * KT));
 #pragma unroll
     for (int o = S::LPE; o < 32; o <<= 1)
 #pragma unroll
@@ -210,6 +227,18 @@ __global__ void __launch_bounds__(kThreads) batch_back_kernel(int64_t n, int K, 
     if (red[i] != 0.0) atomicAdd(acc + f0 + i, red[i]);
 }
 
+// Xt[j*t + f'] = X[j*K + f0 + f'], the tile's frames of every image row
+// (t a multiple of 4: one 16-byte copy per thread and step).
+__global__ void batch_tile_images_kernel(int64_t n, int K, int f0, int t, const float* __restrict__ X,
+                                         float* __restrict__ Xt) {
+  const int q = t / 4;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n * q; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t j = i / q;
+    const int v = int(i - j * q) * 4;
+    *reinterpret_cast<float4*>(Xt + j * t + v) = *reinterpret_cast<const float4*>(X + j * K + f0 + v);
+  }
+}
+
 // X = XX * (1 / acc[f]) for all frames; then acc = 0 for the next pass.
 __global__ void batch_normalise_kernel(int64_t n, int K, float* __restrict__ X, const float* __restrict__ XX,
                                        const double* __restrict__ acc) {
@@ -229,14 +258,25 @@ struct BackGroup {
 template <int KT, typename VT>
 cudaError_t launch_tile(const BatchArgs& a, bool forward, int f0, double* acc, unsigned long long* next,
                         const BackGroup& grp, cudaStream_t s) {
-  if (forward)
+  if (forward) {
+    const bool compact = a.Xt && KT < a.K;
+    if (compact) {
+      int64_t blocks = (a.n * (KT / 4) + kThreads - 1) / kThreads;
+      if (blocks > 148 * 8) blocks = 148 * 8;
+      batch_tile_images_kernel<<<unsigned(std::max<int64_t>(blocks, 1)), kThreads, 0, s>>>(a.n, a.K, f0, KT, a.X,
+                                                                                         a.Xt);
+      note_launches(1);
+    }
     batch_forward_kernel<KT, VT><<<grid_warps(a.m), kThreads, 0, s>>>(
-        a.m, a.K, f0, a.rp, a.col, static_cast<const VT*>(a.val), a.half ? a.rscale : nullptr, a.Y, a.X, a.rank, a.E);
-  else
+        a.m, a.K, f0, a.rp, a.col, static_cast<const VT*>(a.val), a.half ? a.rscale : nullptr, a.Y,
+        compact ? a.Xt : a.X + f0, compact ? KT : a.K, a.rank, a.E + int64_t(f0) * a.m);
+  } else {
     batch_back_kernel<KT, VT><<<unsigned((a.n + kColsPerWarp * (kThreads / 32) - 1) / (kColsPerWarp * (kThreads / 32))),
-                                kThreads, 0, s>>>(a.n, a.K, f0, next, a.cp, a.trow, static_cast<const VT*>(a.tval), a.E,
+                                kThreads, 0, s>>>(a.n, a.K, f0, next, a.cp, a.trow, static_cast<const VT*>(a.tval),
+                                                  a.E + int64_t(f0) * a.m,
                                                   a.X, a.S, a.col_order, a.XX, acc, grp.mode ? a.seg : nullptr,
                                                   a.seg_blocks + 1, grp.b0, grp.b1, grp.mode, a.P);
+  }
   note_launches(1);
   return cudaGetLastError();
 }
