@@ -308,7 +308,7 @@ void raptr_server::drop(Entry* e) {
 
 // Lays the batch out again for its current requests: K = the smallest
 // multiple of 4 that holds them (the batch kernels run any such K in tiles
-// of at most 32 frames, so at most 3 slots are padding, which repeat slot
+// of at most 64 frames, so at most 3 slots are padding, which repeat slot
 // 0).  The arrays are reused; only a batch that outgrows them allocates
 // (the next power of two of frames, up to max_frames), so requests joining
 // and leaving do not allocate or synchronise.
@@ -504,9 +504,10 @@ void raptr_server::loop() {
         e->launch_status = RAPTR_ERR_NOMEM;
         e->launch_error = "batch relayout failed";
       } else {
-        // all frames in sweeps of at most 32 (a multiple of 4 frames)
+        // all frames in sweeps of at most 64 (a multiple of 4 frames): one
+        // 64-frame sweep takes 112 ms at 70^3, two of 32 take 120 ms
         e->launch_status = raptr_mlem_batch(e->ctx, e->m, e->n, e->K, 1, e->rp, e->col, e->hval, e->rscale, e->cp,
-                                            e->trow, e->htval, e->rank, e->Y, e->s, e->X(), 1, 32, nullptr,
+                                            e->trow, e->htval, e->rank, e->Y, e->s, e->X(), 1, 64, nullptr,
                                             e->stream);
         if (e->launch_status != RAPTR_OK) e->launch_error = raptr_last_error();
       }
