@@ -1665,7 +1665,7 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
                                           size_t(n) * n_frames * sizeof(float), size_t(n_frames) * sizeof(double),
                                           size_t(n_frames) * sizeof(unsigned long long) * kBatchRowBlocks,
                                           size_t(n) * std::min(kt, int(n_frames)) * sizeof(float),
-                                          size_t(n) * std::min(kt, int(n_frames)) * sizeof(float)})));
+                                          size_t(n) * batch_tile_at(n_frames, kt, 0) * sizeof(float)})));
   Carve cv(ctx->d_scratch);
   // the tube order of the back pass applies when the columns are the
   // context's voxels
@@ -1674,8 +1674,10 @@ raptr_status raptr_mlem_batch(raptr_ctx* ctx, int64_t m, int64_t n, int32_t n_fr
   a.XX = cv.take<float>(size_t(n) * n_frames);
   double* acc = cv.take<double>(size_t(n_frames));
   unsigned long long* next = cv.take<unsigned long long>(size_t(n_frames) * kBatchRowBlocks);
-  // the compact images of a tile narrower than the batch
-  if (std::min(kt, int(n_frames)) < n_frames) a.Xt = cv.take<float>(size_t(n) * std::min(kt, int(n_frames)));
+  // the compact images of a tile narrower than the batch (the first tile
+  // is the widest: 12 frames at kt = 64 run as 8 + 4)
+  const int widest = batch_tile_at(n_frames, kt, 0);
+  if (widest < n_frames) a.Xt = cv.take<float>(size_t(n) * widest);
   // the back pass in row-block groups when one tile's ratios exceed L2
   if (m > 0 && double(m) * std::min(kt, int(n_frames)) * sizeof(float) > kBatchBlockingBytes) {
     RCU(ctx->block_seg(d_col_ptr, d_row_idx, m, n, s, &a.seg));

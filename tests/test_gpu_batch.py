@@ -13,7 +13,7 @@ from raptr_b200 import config as cfg
 pytestmark = pytest.mark.gpu
 
 SEED = 1251
-K = 8
+K = 12
 FRAME_RTOL = 1e-5  # batched vs single-frame image (relative L2); summation order differs
 F64_RTOL = {False: 1e-4, True: 1e-3}  # vs the FP64 oracle: FP32 matrix, FP16 matrix
 K64 = 64
@@ -47,8 +47,11 @@ def frames(rlib, torch):
 
 
 @pytest.mark.parametrize("half", [False, True])
-@pytest.mark.parametrize("tile", [4, 8])
+@pytest.mark.parametrize("tile", [4, 8, 64])
 def test_batch_equals_single_frames(rlib, torch, frames, half, tile):
+    """Each frame of the batch equals its own single-frame iteration; with
+    tile 64 the 12 frames run as tiles of 8 and 4 narrower than the batch
+    (their images gathered from a compact copy, as at tiles 4 and 8)."""
     ctx, A, Y = frames
     n = A.n
     s = (rlib.sensitivity_half(A) if half else rlib.sensitivity(A))[1]
