@@ -822,12 +822,90 @@ __global__ void __launch_bounds__(T) sm_dense_kernel(DGeom g, const float2* __re
     if (tid == 0) row_nnz[blockIdx.x] = total;
     return;
   }
+  // z slabs: the entries ascend in z slab by slab, within a slab in (x, y).
+  // Column order is (x, y, z): a counting sort by (x, y) over the box that
+  // holds every slab's window places them, an entry's rank among the
+  // entries of its (x, y) being the number of their z below its own (a z
+  // bitmask per key).  When the box's counters do not fit beside the row's
+  // staging in shared memory (or the grid has more than 96 z planes), the
+  // bitonic sort does it.
+  __shared__ int zbox[4];
+  if (tid == 0) {
+    zbox[0] = INT_MAX;
+    zbox[1] = INT_MIN;
+    zbox[2] = INT_MAX;
+    zbox[3] = INT_MIN;
+  }
   __syncthreads();
+  for (int sl = tid; sl < na; sl += T) {
+    atomicMin(&zbox[0], ulo[sl]);
+    atomicMax(&zbox[1], ulo[sl] + wu);
+    atomicMin(&zbox[2], vlo[sl]);
+    atomicMax(&zbox[3], vlo[sl] + wv);
+  }
   for (int i = tid; i < total; i += T) {
     keys[i] = st_col[base + i];
     vals[i] = st_val[base + i];
   }
-  sort_and_write<T>(keys, vals, total, st_col, st_val, base, row_nnz + blockIdx.x);
+  __syncthreads();
+  const int wy = zbox[3] - zbox[2];
+  const int nkeys = (zbox[1] - zbox[0]) * wy;
+  constexpr int kKeyBytes = 16;  // counter + 96-bit z mask
+  const int key_cap = int((row_smem_bytes(H) - size_t(H) * 8) / kKeyBytes);
+  if (nkeys > key_cap || nz > 96) {
+    sort_and_write<T>(keys, vals, total, st_col, st_val, base, row_nnz + blockIdx.x);
+    return;
+  }
+  int* cnt = reinterpret_cast<int*>(smem + size_t(H) * 8);
+  unsigned* zmask = reinterpret_cast<unsigned*>(cnt + nkeys);
+  for (int i = tid; i < nkeys * 4; i += T) cnt[i] = 0;  // counters and masks
+  __syncthreads();
+  const int x0 = zbox[0], y0 = zbox[2];
+  for (int i = tid; i < total; i += T) {
+    const int c = keys[i];
+    const int x = c / nyz, r = c - x * nyz, y = r / nz, z = r - y * nz;
+    const int k = (x - x0) * wy + (y - y0);
+    atomicAdd(&cnt[k], 1);
+    atomicOr(&zmask[3 * k + (z >> 5)], 1u << (z & 31));
+  }
+  __syncthreads();
+  // exclusive scan of the counters: each thread a run of consecutive keys
+  {
+    const int per = (nkeys + T - 1) / T;
+    const int k0 = min(tid * per, nkeys), k1 = min(k0 + per, nkeys);
+    int run = 0;
+    for (int k = k0; k < k1; k++) run += cnt[k];
+    int incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[w] = incl;
+    __syncthreads();
+    int wbase = 0;
+    for (int q = 0; q < w; q++) wbase += warp_sums[q];
+    int off = wbase + incl - run;
+    for (int k = k0; k < k1; k++) {
+      const int c = cnt[k];
+      cnt[k] = off;
+      off += c;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < total; i += T) {
+    const int c = keys[i];
+    const int x = c / nyz, r = c - x * nyz, y = r / nz, z = r - y * nz;
+    const int k = (x - x0) * wy + (y - y0);
+    const unsigned* m = zmask + 3 * k;
+    const int zw = z >> 5;
+    int rank = __popc(m[zw] & ((1u << (z & 31)) - 1u));
+    if (zw > 0) rank += __popc(m[0]);
+    if (zw > 1) rank += __popc(m[1]);
+    st_col[base + cnt[k] + rank] = c;
+    st_val[base + cnt[k] + rank] = vals[i];
+  }
+  if (tid == 0) row_nnz[blockIdx.x] = total;
 }
 
 // Table kernel: its rays (generated, or given in `rays`) summed per voxel in
