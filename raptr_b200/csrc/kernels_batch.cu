@@ -153,7 +153,6 @@ __global__ void __launch_bounds__(kThreads, kBatchBlocks) batch_back_kernel(int6
   const int lane = threadIdx.x & 31;
   const int es = lane / S::LPE, fg = lane % S::LPE;
   const int fbase = f0 + fg * S::VEC;
-  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
   // the lane's four frames of this tile's block of ratios
   const float* __restrict__ Et = Eb + fg * S::VEC;
   double fsum[S::VEC];
@@ -162,7 +161,6 @@ __global__ void __launch_bounds__(kThreads, kBatchBlocks) batch_back_kernel(int6
   __shared__ double red[KT];  // the block's image sums per frame of the tile
   for (int i = threadIdx.x; i < KT; i += blockDim.x) red[i] = 0.0;
   __syncthreads();
-  (void)nw;
   for (int taken = 0; taken < kColsPerWarp; taken++) {
     // columns are handed out one at a time (their lengths vary ~20-fold)
     unsigned long long q = 0;
