@@ -572,3 +572,33 @@ def test_matrix_memory_is_released(rlib, torch, ctx_small):
     torch.cuda.synchronize()
     rlib.trim_memory()
     assert torch.cuda.mem_get_info()[0] > free0 - nbytes // 4
+
+
+def test_zslab_rows_both_sort_paths(rlib, oracle, ctx_full):
+    """z-slab rows come out of the dense kernel in column order either by the
+    counting sort over their windows' (x, y) box (at most 1024 keys at
+    H = 4096) or by the bitonic sort (larger boxes): rows of both kinds,
+    chosen with the host restatement of the windows, against the oracle."""
+    from test_slab_windows import boxes, windows
+
+    g = cfg.FULL
+    per = g.n0z * g.n0y * g.n1z * g.n1y
+    rng = np.random.default_rng(31)
+    small_box, large_box = [], []
+    # large boxes: a few % of the z-slab rows near 46-56 degrees, where the
+    # rays drift most in x from slab to slab
+    for a in list(range(23, 29)) * 10 + list(range(40, 50)):
+        for cnl in (a * per + rng.integers(0, per, 6)).tolist():
+            win = windows(g, *boxes(oracle, g, cnl)[:2])
+            if win is None or win[0] != 2:
+                continue
+            rows = win[1]
+            wu = max(r[1] - r[0] + 1 for r in rows)
+            wv = max(r[3] - r[2] + 1 for r in rows)
+            nkeys = (max(r[0] for r in rows) + wu - min(r[0] for r in rows)) * \
+                    (max(r[2] for r in rows) + wv - min(r[2] for r in rows))
+            (small_box if nkeys <= 1024 else large_box).append(cnl)
+    assert len(small_box) >= 8 and len(large_box) >= 6, (len(small_box), len(large_box))
+    lst = np.array(small_box[:24] + large_box[:16], np.int32)
+    A = ctx_full.build(lst, 1000, SEED)
+    assert_rows_equal(*A.to_numpy(), *oracle.sysmat(g, lst, 1000, SEED, method=1))
