@@ -120,8 +120,16 @@ __device__ void load_row_tile(int64_t m, int rows_per_tile, int t, const int64_t
   tile->gstart = sh_gstart;
 }
 
-// Histogram of one pass: hist[d * ntiles + t].  In the first pass (ROWS)
-// also counts columns (colcnt) and checks them.
+// Histogram of one pass: hist[d * ntiles + t].  The first pass (ROWS)
+// checks the columns.  Column counts (colcnt, when given) are taken in the
+// last pass.  With two passes its input is sorted by the low digit, so a
+// tile holds (nearly) one low digit, that of its first entry: its entries
+// of that low digit are counted per high digit in shared memory and added
+// to colcnt once per column at the end; any other entry adds to colcnt
+// directly.  Each thread loads kHistItems entries before counting them, so
+// that their loads are in flight together.
+constexpr int kHistItems = 4;
+
 template <bool ROWS>
 __global__ void __launch_bounds__(kWarps * 32) rs_hist(int64_t m, int64_t n, int rows_per_tile, int64_t nent_flat,
                                                        const int64_t* __restrict__ rp, const int32_t* __restrict__ key,
@@ -129,11 +137,15 @@ __global__ void __launch_bounds__(kWarps * 32) rs_hist(int64_t m, int64_t n, int
                                                        int64_t* __restrict__ hist, int32_t* __restrict__ colcnt,
                                                        int32_t* __restrict__ bad) {
   __shared__ int sh_hist[kRadix];
+  __shared__ int sh_col[kRadix];  // last of two passes: counts of the first entry's low digit
   __shared__ int sh_start[kMaxTileRows + 1];
   __shared__ int64_t sh_gstart[kMaxTileRows];
   __shared__ int sh_len[kMaxTileRows];
   const int t = blockIdx.x;
-  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) sh_hist[d] = 0;
+  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+    sh_hist[d] = 0;
+    sh_col[d] = 0;
+  }
   RowTile tile{};
   int64_t e0 = 0;
   int nent;
@@ -145,26 +157,53 @@ __global__ void __launch_bounds__(kWarps * 32) rs_hist(int64_t m, int64_t n, int
     nent = int(nent_flat - e0 < kTileEntries ? nent_flat - e0 : kTileEntries);
     __syncthreads();
   }
-  for (int e = threadIdx.x; e < nent; e += blockDim.x) {
-    int64_t q;
-    if (ROWS) {
-      int i;
-      tile.locate(e, &i, &q);
-    } else {
-      q = e0 + e;
-    }
-    const int c = __ldg(key + q);
-    if (ROWS) {
-      if (c < 0 || c >= n) {
-        atomicOr(bad, 1);
-        continue;
+  const int lmask = (1 << shift) - 1;
+  const int low0 = (!ROWS && colcnt && nent > 0) ? (__ldg(key + e0) & lmask) : 0;
+  int row = -1;  // ROWS: row of this thread's previous entry
+  for (int b = threadIdx.x; b < nent; b += kHistItems * blockDim.x) {
+    int c[kHistItems];
+#pragma unroll
+    for (int u = 0; u < kHistItems; u++) {
+      const int e = b + u * int(blockDim.x);
+      c[u] = 0;
+      if (e < nent) {
+        int64_t q;
+        if (ROWS) {
+          if (row < 0)
+            tile.locate(e, &row, &q);
+          else
+            tile.advance(e, &row, &q);
+        } else {
+          q = e0 + e;
+        }
+        c[u] = __ldg(key + q);
       }
-      atomicAdd(colcnt + c, 1);
     }
-    atomicAdd(sh_hist + ((c >> shift) & mask), 1);
+#pragma unroll
+    for (int u = 0; u < kHistItems; u++) {
+      if (b + u * int(blockDim.x) >= nent) break;
+      const int cu = c[u];
+      const int d = (cu >> shift) & mask;
+      if (ROWS) {
+        if (cu < 0 || cu >= n) {
+          atomicOr(bad, 1);
+          continue;
+        }
+        if (colcnt) atomicAdd(colcnt + cu, 1);
+      } else if (colcnt) {
+        if ((cu & lmask) == low0)
+          atomicAdd(sh_col + d, 1);
+        else
+          atomicAdd(colcnt + cu, 1);
+      }
+      atomicAdd(sh_hist + d, 1);
+    }
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[int64_t(d) * ntiles + t] = sh_hist[d];
+  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+    hist[int64_t(d) * ntiles + t] = sh_hist[d];
+    if (!ROWS && colcnt && sh_col[d] > 0) atomicAdd(colcnt + ((d << shift) | low0), sh_col[d]);
+  }
 }
 
 // Scatter of one pass.  Positions: off[d * ntiles + t] + rank of the entry
@@ -216,30 +255,40 @@ __global__ void __launch_bounds__(kWarps * 32, 1) rs_scatter(int64_t m, int64_t 
     int dig[kItems], rnk[kItems], kk[kItems];
     int kv[kItems];
     float vv[kItems];
-    int row = -1;  // ROWS: row of this lane's previous item
-    // load and rank within the warp, items in order
+    // load the lane's items first, so that their loads are in flight
+    // together, then rank them within the warp in order
+    {
+      int row = -1;  // ROWS: row of this lane's previous item
+#pragma unroll
+      for (int it = 0; it < kItems; it++) {
+        const int e = c0 + w * (kItems * 32) + it * 32 + lane;
+        int c = 0, k = 0;
+        float v = 0.f;
+        if (e < nent) {
+          int64_t q;
+          if (ROWS) {
+            if (row < 0)
+              tile.locate(e, &row, &q);
+            else
+              tile.advance(e, &row, &q);
+            k = int(tile.k0 + row);
+          } else {
+            q = e0 + e;
+            k = __ldg(kin + q);
+          }
+          c = __ldg(key + q);
+          v = __ldg(vin + q);
+        }
+        kk[it] = c;
+        kv[it] = k;
+        vv[it] = v;
+      }
+    }
 #pragma unroll
     for (int it = 0; it < kItems; it++) {
-      const int e = c0 + w * (kItems * 32) + it * 32 + lane;
-      const bool valid = e < nent;
-      int c = 0, k = 0;
-      float v = 0.f;
-      if (valid) {
-        int64_t q;
-        if (ROWS) {
-          if (row < 0)
-            tile.locate(e, &row, &q);
-          else
-            tile.advance(e, &row, &q);
-          k = int(tile.k0 + row);
-        } else {
-          q = e0 + e;
-          k = __ldg(kin + q);
-        }
-        c = __ldg(key + q);
-        v = __ldg(vin + q);
-        if (c < 0 || c >= n) c = 0;  // flagged by the histogram pass
-      }
+      const bool valid = c0 + w * (kItems * 32) + it * 32 + lane < nent;
+      int c = kk[it];
+      if (c < 0 || c >= n) c = 0;  // flagged by the histogram pass
       const int d = valid ? (c >> shift) & mask : -1;
       const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : kRadix + lane);
       const int r = __popc(peers & lanemask_lt());
@@ -251,8 +300,6 @@ __global__ void __launch_bounds__(kWarps * 32, 1) rs_scatter(int64_t m, int64_t 
       dig[it] = d;
       rnk[it] = base + r;
       kk[it] = c;
-      kv[it] = k;
-      vv[it] = v;
     }
     __syncthreads();
     // per digit (one per thread): exclusive prefix over the warps, chunk
@@ -382,7 +429,9 @@ cudaError_t launch_transpose_radix(const RadixPlan& p, int64_t m, int64_t n, int
   const int nt1 = int(p.ntiles_rows);
   const int64_t h1 = int64_t(kRadix) * nt1;
   const int m1 = (1 << p.bits1) - 1;
-  rs_hist<true><<<nt1, kWarps * 32, 0, s>>>(m, n, p.rows_per_tile, 0, rp, col, order, 0, m1, nt1, hist, colcnt, bad);
+  // column counts in the last pass (see rs_hist)
+  rs_hist<true><<<nt1, kWarps * 32, 0, s>>>(m, n, p.rows_per_tile, 0, rp, col, order, 0, m1, nt1, hist,
+                                            p.passes == 1 ? colcnt : nullptr, bad);
   note_launches(1);
   if ((e = launch_scan_i64(hist, h1, off, scan_tmp, s)) != cudaSuccess) return e;
   if (p.passes == 1) {
@@ -396,7 +445,7 @@ cudaError_t launch_transpose_radix(const RadixPlan& p, int64_t m, int64_t n, int
     const int nt2 = int(p.ntiles_flat);
     const int64_t h2 = int64_t(kRadix) * nt2;
     rs_hist<false><<<nt2, kWarps * 32, 0, s>>>(m, n, 0, nnz, nullptr, st_key, nullptr, p.bits1, kRadix - 1, nt2,
-                                               hist, nullptr, bad);
+                                               hist, colcnt, bad);
     note_launches(1);
     if ((e = launch_scan_i64(hist, h2, off, scan_tmp, s)) != cudaSuccess) return e;
     rs_scatter<false><<<nt2, kWarps * 32, sm2, s>>>(m, n, 0, nnz, nullptr, st_key, st_k, st_v, nullptr, p.bits1,

@@ -41,7 +41,9 @@ def random_csr(rng, m, n, density, sort_rows=True):
             np.concatenate(vals).astype(np.float32) if vals else np.zeros(0, np.float32))
 
 
-@pytest.mark.parametrize("n,sort_rows", [(700, True), (700, False), (5000, True), (5000, False), (300000, True)])
+# n = 700: one pass; 5000 and 300000: a 9-bit first digit; 800000: two 10-bit digits
+@pytest.mark.parametrize("n,sort_rows",
+                         [(700, True), (700, False), (5000, True), (5000, False), (300000, True), (800000, True)])
 def test_transpose_general_csr(rlib, torch, n, sort_rows):
     rng = np.random.default_rng(n + sort_rows)
     m = 3000
