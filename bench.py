@@ -287,11 +287,11 @@ def synth_measurement(R, torch, ctx, w, lst, dist=None):
     return cfg.poisson_measurement(lam.cpu().numpy(), w["counts"], MEAS_SEED)
 
 
-def run_job(R, torch, ctx, w, lst, y_dev, dist=None, keep=False):
-    """One reconstruction job; returns per-phase device times (ms), and with
-    keep the matrix and the inputs of its iterations (for kernel timing
-    after the timed region).  On one GPU the iterations run as one CUDA
-    graph."""
+def run_job(R, torch, ctx, w, lst, y_dev, dist=None):
+    """One reconstruction job; returns per-phase device times (ms) and the
+    device time of every forward and back pass of its iterations (CUDA
+    events between the passes, on the stream they are launched on: stream
+    launches, which run the iterations as fast as one CUDA graph of them)."""
     g = w["geom"]
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
     ev[0].record()
@@ -310,7 +310,7 @@ def run_job(R, torch, ctx, w, lst, y_dev, dist=None, keep=False):
     x = torch.full((g.n_voxels,), np.float32(1.0 / g.n_voxels), device="cuda")
     kt = None
     if dist is None:
-        ctx.mlem(A, y_dev, s, x, w["niter"], use_graph=True)
+        kt = ctx.mlem(A, y_dev, s, x, w["niter"], use_graph=False, kernel_times=True)
     else:
         ops = sharded.ops
         kev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(w["niter"])]
@@ -328,8 +328,6 @@ def run_job(R, torch, ctx, w, lst, y_dev, dist=None, keep=False):
     torch.cuda.synchronize()
     t = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
     info = {"nnz": A.nnz, "m": A.m}
-    if keep:
-        info.update({"A": A, "s": s})
     del A  # freed by reference count (its blocks go back to the library's cache)
     return {"build_ms": t[0], "transpose_ms": t[1], "sens_ms": t[2], "mlem_ms": t[3], "job_ms": sum(t),
             "kernel_ms": kt, "x": x, **info}
@@ -657,20 +655,12 @@ def main():
     t_end = torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("raptr_timed_steps")
     t_start.record()
-    steps = [run_job(R, torch, ctx, w, lst, y_dev, dist, keep=(i == args.steps - 1)) for i in range(args.steps)]
+    steps = [run_job(R, torch, ctx, w, lst, y_dev, dist) for i in range(args.steps)]
     t_end.record()
     torch.cuda.nvtx.range_pop()
     barrier()
     launches = R.kernel_launches() - launches0
     clocks = sampler.stop()
-    # per-pass device times of the iteration, on the last step's matrix,
-    # outside the timed region (events between the passes)
-    last = steps[-1]
-    if dist is None and "A" in last:
-        last["kernel_ms"] = ctx.mlem(last["A"], y_dev, last["s"], last["x"].clone(), 10, use_graph=False,
-                                     kernel_times=True)
-    last.pop("A", None)
-    last.pop("s", None)
     gc.collect()
     total_ms = t_start.elapsed_time(t_end)
     if dist is not None:
