@@ -655,7 +655,7 @@ def main():
     t_end = torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("raptr_timed_steps")
     t_start.record()
-    steps = [run_job(R, torch, ctx, w, lst, y_dev, dist) for i in range(args.steps)]
+    steps = [run_job(R, torch, ctx, w, lst, y_dev, dist) for _ in range(args.steps)]
     t_end.record()
     torch.cuda.nvtx.range_pop()
     barrier()
