@@ -13,7 +13,7 @@
 // different digits); the second pass stores directly.  The first pass reads
 // the CSR rows directly (a tile is a range of positions k); the second reads
 // the staging written by the first and writes the CSC.  Column pointers come
-// from a column histogram taken during the first pass.
+// from column counts taken in the last pass's histogram.
 //
 // Scales as (passes x 3) streaming sweeps of the entries; used for matrices
 // whose columns fit two passes (n <= 2^20).  The first digit is 9 bits
