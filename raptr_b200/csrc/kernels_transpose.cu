@@ -52,8 +52,9 @@ struct RowTile {
   const int64_t* gstart;  // nrows global starts (into col / val)
 
   // tile-local entry e >= start[i] -> the row holding it, scanning forward
-  // from row i (a lane's successive entries are 32 apart, mostly in the
-  // same row)
+  // from row i (a thread's successive entries are close: 32 apart in a
+  // scatter chunk, mostly in the same row; one block apart in a histogram,
+  // a row or two on)
   __device__ __forceinline__ void advance(int e, int* i, int64_t* q) const {
     int r = *i;
     while (start[r + 1] <= e) r++;
