@@ -550,6 +550,54 @@ def test_full_size_matrix_properties(rlib, oracle, torch, ctx_full):
     assert abs(float(s64.sum()) - total) <= 1e-9 * total
 
 
+def test_full_size_transpose_properties(rlib, torch, ctx_full):
+    """The transpose of the whole 70^3 x 5.14M-channel matrix (3.7e9
+    entries, both radix passes): the column pointers are the column counts
+    of the rows, row positions ascend within every column, the values sum
+    as the rows' do, the rows sampled by the test above (checked against
+    the oracle there) sit entry by entry in their columns with the same
+    bits, and the FP64 column sums through the transpose equal those through
+    the rows (size-independent checks)."""
+    g = cfg.FULL
+    A = ctx_full.build(np.arange(g.n_channels, dtype=np.int32), 1000, SEED)
+    s_rows, _ = rlib.sensitivity(A, use_transpose=False)
+    A.transpose()
+    m, n, nnz = A.m, A.n, A.nnz
+    cp = A.col_ptr
+    assert int(cp[0]) == 0 and int(cp[-1]) == nnz
+    chunk = 1 << 28
+    counts = torch.zeros(n, dtype=torch.int64, device="cuda")
+    total = ttotal = 0.0
+    starts = cp[1:-1]
+    for i in range(0, nnz, chunk):
+        j = min(i + chunk, nnz)
+        counts += torch.bincount(A.col[i:j].long(), minlength=n)
+        total += float(A.val[i:j].double().sum())
+        ttotal += float(A.tval[i:j].double().sum())
+        ri = A.row_idx[i:min(j + 1, nnz)]  # one entry of overlap with the next chunk
+        assert int(ri.min()) >= 0 and int(ri.max()) < m
+        # a position not above its predecessor may only open a column
+        desc = torch.nonzero(ri[1:] <= ri[:-1]).squeeze(1) + (i + 1)
+        assert bool(torch.isin(desc, starts).all())
+    assert torch.equal(cp[1:] - cp[:-1], counts)
+    assert abs(ttotal - total) <= 1e-9 * total
+    rng = np.random.Generator(np.random.PCG64(77))
+    sample = np.sort(rng.choice(g.n_channels, 64, replace=False))
+    for r in sample[:32]:
+        b, e = int(A.row_ptr[r]), int(A.row_ptr[r + 1])
+        cols = A.col[b:e].long()
+        lo, lens = cp[cols], cp[cols + 1] - cp[cols]
+        seg = torch.repeat_interleave(torch.arange(cols.numel(), device="cuda"), lens)
+        idx = torch.arange(int(lens.sum()), device="cuda") + torch.repeat_interleave(lo - (torch.cumsum(lens, 0) - lens),
+                                                                                       lens)
+        hit = torch.nonzero(A.row_idx[idx] == int(A.row_rank[r])).squeeze(1)
+        assert torch.equal(seg[hit], torch.arange(cols.numel(), device="cuda"))  # once in each of its columns
+        assert torch.equal(A.tval[idx[hit]].view(torch.int32), A.val[b:e].view(torch.int32))
+    s_csc, _ = rlib.sensitivity(A)
+    assert torch.equal(s_csc == 0, s_rows == 0)
+    assert float(((s_csc - s_rows).abs() / s_rows.clamp_min(1e-300)).max()) <= 1e-10
+
+
 def test_matrix_memory_is_released(rlib, torch, ctx_small):
     """Device memory of a matrix (and its transpose) is returned once the
     Matrix and its tensor views are dropped: to the library's block cache,
