@@ -346,12 +346,15 @@ struct Builder {
   int64_t rows_done = 0;
 
   // Builds rows [row0, row0+nrows) at `level` as a pipeline of chunks: the
-  // row kernel of chunk i+1 runs on the caller's stream while chunk i is
-  // placed (scan, capacity, gather) on a second stream, from a second
-  // staging buffer, so the device does not idle while the host reads a
-  // chunk's flags and entry count.  A chunk whose table overflowed drains
-  // the pipeline, is rebuilt at the next level by rows(), and the pipeline
-  // restarts after it.
+  // row kernel of chunk i+1 runs while chunk i is placed (scan, capacity,
+  // gather) on a placement stream, from a second staging buffer, so the
+  // device does not idle while the host reads a chunk's flags and entry
+  // count.  Even chunks run on the caller's stream and odd ones on a second
+  // row stream, so that a chunk's CTAs fill the SMs as the previous chunk's
+  // last ones retire (one stream would leave its last wave draining alone);
+  // a chunk waits for the placement of the chunk two before it, which used
+  // its buffer.  A chunk whose table overflowed drains the pipeline, is
+  // rebuilt at the next level by rows(), and the pipeline restarts after it.
   raptr_status rows_pipelined(int level, int64_t row0, int64_t nrows) {
     const int H = sm_level_capacity(level);
     int64_t per = std::max<int64_t>(1, int64_t(kStagingBudget / (size_t(H) * 8)));
@@ -360,19 +363,21 @@ struct Builder {
     // words 0-1: the dense kernel's flags, 2-3: the table kernel's (per buffer)
     volatile int32_t* h_flags = reinterpret_cast<volatile int32_t*>(ctx->h_pin);
     volatile int64_t* h_total = ctx->h_pin + 2;
-    cudaStream_t P = nullptr;
+    cudaStream_t P = nullptr, S2 = nullptr;
     cudaEvent_t ev_k[2] = {nullptr, nullptr}, ev_g[2] = {nullptr, nullptr}, ev_j = nullptr;
     auto release = [&]() {
       for (auto e : ev_k) if (e) cudaEventDestroy(e);
       for (auto e : ev_g) if (e) cudaEventDestroy(e);
       if (ev_j) cudaEventDestroy(ev_j);
       if (P) cudaStreamDestroy(P);
+      if (S2) cudaStreamDestroy(S2);
     };
     struct Guard {
       std::function<void()> f;
       ~Guard() { f(); }
     } guard{release};
     RCU(cudaStreamCreateWithFlags(&P, cudaStreamNonBlocking));
+    RCU(cudaStreamCreateWithFlags(&S2, cudaStreamNonBlocking));
     for (int b = 0; b < 2; b++) {
       RCU(cudaEventCreateWithFlags(&ev_k[b], cudaEventDisableTiming));
       RCU(cudaEventCreateWithFlags(&ev_g[b], cudaEventDisableTiming));
@@ -380,8 +385,9 @@ struct Builder {
     RCU(cudaEventCreateWithFlags(&ev_j, cudaEventDisableTiming));
     auto drain = [&]() -> cudaError_t {
       cudaError_t e = cudaStreamSynchronize(s);
-      cudaError_t e2 = cudaStreamSynchronize(P);
-      return e != cudaSuccess ? e : e2;
+      cudaError_t e2 = cudaStreamSynchronize(S2);
+      cudaError_t e3 = cudaStreamSynchronize(P);
+      return e != cudaSuccess ? e : (e2 != cudaSuccess ? e2 : e3);
     };
     const int64_t end = row0 + nrows;
     int64_t r0 = row0;
@@ -400,22 +406,25 @@ struct Builder {
         st_val[b] = cv.take<float>(size_t(per) * H);
         row_nnz[b] = cv.take<int32_t>(size_t(per));
       }
-      // placement starts after the caller's earlier work
+      // placement and the second row stream start after the caller's
+      // earlier work
       RCU(cudaEventRecord(ev_j, s));
       RCU(cudaStreamWaitEvent(P, ev_j, 0));
+      RCU(cudaStreamWaitEvent(S2, ev_j, 0));
       auto launch = [&](int64_t i) -> cudaError_t {
         const int b = int(i & 1);
+        cudaStream_t q = b ? S2 : s;  // buffer b's chunks, in order, on one stream
         const int64_t r = r0 + i * per, k = std::min(per, end - r);
         cudaError_t e = cudaSuccess;
-        if (i >= 2) e = cudaStreamWaitEvent(s, ev_g[b], 0);  // chunk i-2 has left this buffer
-        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_flags + b, 0, sizeof(int32_t), s);
+        if (i >= 2) e = cudaStreamWaitEvent(q, ev_g[b], 0);  // chunk i-2 has left this buffer
+        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_flags + b, 0, sizeof(int32_t), q);
         if (e == cudaSuccess)
           e = launch_sm_rows(level, ctx->dg, ctx->d_sincos, d_cnl, r, k, nrays, seed, d_rays, st_col[b], st_val[b],
-                             row_nnz[b], ctx->d_flags + b, s, ctx->d_flags + 4, d_rays ? kRowsAll : kRowsDense);
+                             row_nnz[b], ctx->d_flags + b, q, ctx->d_flags + 4, d_rays ? kRowsAll : kRowsDense);
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(const_cast<int32_t*>(h_flags) + b, ctx->d_flags + b, sizeof(int32_t),
-                              cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaEventRecord(ev_k[b], s);
+                              cudaMemcpyDeviceToHost, q);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_k[b], q);
         return e;
       };
       cudaError_t e = launch(0);
