@@ -112,30 +112,53 @@ class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # the memory clock and HBM temperature, from a second process so that a
+    # field a driver does not know costs only these: the HBM-bound passes
+    # run ~5 % apart on different boxes at the same SM clock
+    EXTRA = "clocks.mem,clocks.max.mem,temperature.memory"
 
     def __init__(self, gpu_id: str):
         self.gpu_id = gpu_id
-        self.proc = None
+        self.proc = self.proc_extra = None
         self.t0 = self.t1 = None
 
-    def start(self):
+    def _spawn(self, fields):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200", "-i",
+            return subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={fields}", "--format=csv,noheader,nounits", "-lms", "200", "-i",
                  self.gpu_id], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
-            self.proc = None
+            return None
+
+    @staticmethod
+    def _collect(proc):
+        if proc is None:
+            return ""
+        proc.terminate()
+        try:
+            out, _ = proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            proc.kill()
+            out, _ = proc.communicate()
+        return out
+
+    def start(self):
+        self.proc = self._spawn(self.FIELDS)
+        self.proc_extra = self._spawn(self.EXTRA)
 
     def stop(self):
+        extra_out = self._collect(self.proc_extra)
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            out, _ = self.proc.communicate(timeout=10)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-            out, _ = self.proc.communicate()
+        out = self._collect(self.proc)
         sm, smax, reasons, power = [], [], set(), []
+        extra = {"mem_mhz": [], "mem_max_mhz": [], "hbm_temp_c": []}
+        for line in extra_out.splitlines():
+            for k, v in zip(extra, (x.strip() for x in line.split(","))):
+                try:
+                    extra[k].append(float(v))
+                except ValueError:  # "N/A" on parts that do not report it
+                    pass
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in out.splitlines():
             f = [x.strip() for x in line.split(",")]
@@ -153,8 +176,15 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         loaded = [s for s, p in zip(sm, power) if p > 0.25 * max(power)] or sm
-        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm), "power_w_max": max(power)}
+        rec = {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+               "samples": len(sm), "power_w_max": max(power)}
+        if extra["mem_mhz"]:
+            rec["mem_mhz"] = statistics.median(extra["mem_mhz"])
+        if extra["mem_max_mhz"]:
+            rec["mem_max_mhz"] = max(extra["mem_max_mhz"])
+        if extra["hbm_temp_c"]:
+            rec["hbm_temp_c_max"] = max(extra["hbm_temp_c"])
+        return rec
 
 
 def gpu_id_for(torch, dev):
